@@ -1,0 +1,303 @@
+"""illcrawl_b200 -- B200 (sm_100a) backend for illcrawl's volumetric projection path.
+
+Python-side view of the C ABI (``include/ilc.h``), used by the tests and the
+benchmark. Names follow the reference's interfaces:
+
+* :class:`Nn8Backend` -- ``reconstruction_backend`` / ``reconstruction_backends::nn8``
+  (reconstruction_backend.hpp:35-58, volumetric_reconstruction_backend_nn8.hpp:36-82)
+* :func:`create_projection` -- ``volumetric_integration::create_projection``
+  (volumetric_integration.cpp:32-88)
+* :func:`xray_flux`, :func:`xray_spectral_flux`, :func:`mean_temperature` -- the
+  quantity kernels of quantities.cl
+* :func:`load_gaunt_table` -- ``util::data_table_loader`` on gaunt_factor.dat
+  (data_table_loader.hpp:39-97)
+
+All compute runs in ``libilcuda.so``; nothing here falls back to the CPU.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import (CONTROLLER_FP64, CONTROLLER_REF32, DA_INVERSE_RANGE, DA_PIXEL_AREA, DA_UNIT,
+                   Camera, IlcError, LosScaling, RenderStats, Tolerance)
+
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+GAUNT_FILE = os.path.join(DATA_DIR, "gaunt_factor.dat")
+
+# Reference defaults (illcrawl_app.hpp:140-143, 197-199)
+REDSHIFT = 0.2
+LUMINOSITY_DISTANCE = 978500.0
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):  # torch tensor on the device
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _is_dev(a):
+    return 1 if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False) else 0
+
+
+def load_gaunt_table(path=GAUNT_FILE):
+    """Parses a whitespace table, skipping lines that start with '#', as
+    util::data_table_loader does (data_table_loader.hpp:39-97). Returns a
+    (rows, columns) float32 array: rows = log(u), columns = log(gamma^2)."""
+    rows = []
+    width = None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("#") or len(line.rstrip("\n")) == 0:
+                continue
+            vals = line.split()
+            if width is None:
+                width = len(vals)
+            elif len(vals) != width:
+                raise ValueError(f"invalid row in {path}: expected {width} entries")
+            rows.append([np.float32(v) for v in vals])
+    return np.asarray(rows, np.float32)
+
+
+def camera(position, look_at, roll, screen_width, num_pix_x, num_pix_y):
+    c = Camera()
+    c.position[:] = [float(v) for v in position]
+    c.look_at[:] = [float(v) for v in look_at]
+    c.roll, c.screen_width = float(roll), float(screen_width)
+    c.num_pix_x, c.num_pix_y = int(num_pix_x), int(num_pix_y)
+    return c
+
+
+def camera_plane(cam):
+    out = np.zeros(13, np.float32)
+    st = _lib.load().ilc_camera_plane(ctypes.byref(cam), _ptr(out))
+    if st:
+        raise IlcError(st, "invalid camera")
+    return out
+
+
+def los_scale(cam, z_range, length_conversion=1.0, area_conversion=1.0, dA_mode=DA_PIXEL_AREA):
+    s = LosScaling(length_conversion, area_conversion, dA_mode)
+    return np.float32(_lib.load().ilc_los_scale(ctypes.byref(cam), z_range, ctypes.byref(s)))
+
+
+class Context:
+    """One device context (stream, grid, Gaunt table, scratch) -- ilc_ctx."""
+
+    def __init__(self, device=0):
+        self.L = _lib.load()
+        self.h = self.L.ilc_create(int(device))
+        if not self.h:
+            raise RuntimeError(f"ilc_create({device}) failed: no usable CUDA device")
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ilc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def check(self, st):
+        if st != _lib.ILC_OK:
+            raise IlcError(st, self.L.ilc_last_error(self.h).decode())
+
+    @property
+    def stream(self):
+        return self.L.ilc_get_stream(self.h)
+
+    def set_step_limit(self, n):
+        self.check(self.L.ilc_set_step_limit(self.h, int(n)))
+
+    # ---- grid / nn8
+    def setup_particles(self, xyzq):
+        if not _is_dev(xyzq):
+            xyzq = np.ascontiguousarray(xyzq, np.float32).reshape(-1, 4)
+        n = xyzq.shape[0]
+        self.check(self.L.ilc_nn8_setup_particles(self.h, _ptr(xyzq), n, _is_dev(xyzq)))
+
+    def grid_describe(self):
+        d = _lib.GridDesc()
+        self.check(self.L.ilc_grid_describe(self.h, ctypes.byref(d)))
+        return {"min_corner": np.array(d.min_corner, np.float32),
+                "cell_sizes": np.array(d.cell_sizes, np.float32),
+                "num_cells": np.array(d.num_cells, np.int32),
+                "total_cells": int(d.total_cells), "num_particles": int(d.num_particles)}
+
+    def grid_export(self):
+        d = self.grid_describe()
+        n = d["num_particles"]
+        cells = np.zeros((d["total_cells"], 2), np.int32)
+        s2u = np.zeros(n, np.uint32)
+        srt = np.zeros((n, 4), np.float32)
+        self.check(self.L.ilc_grid_export(self.h, _ptr(cells), _ptr(s2u), _ptr(srt), 0))
+        return cells, s2u, srt
+
+    def nn8_query(self, points, merge_previous=False, slots=False):
+        dev = _is_dev(points)
+        if not dev:
+            points = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
+        n = points.shape[0]
+        if dev:
+            import torch
+            out = torch.empty(n, dtype=torch.float32, device=points.device)
+            idx = torch.empty((n, 8), dtype=torch.int32, device=points.device) if slots else None
+            d8 = torch.empty((n, 8), dtype=torch.float32, device=points.device) if slots else None
+        else:
+            out = np.zeros(n, np.float32)
+            idx = np.zeros((n, 8), np.int32) if slots else None
+            d8 = np.zeros((n, 8), np.float32) if slots else None
+        self.check(self.L.ilc_nn8_query(self.h, _ptr(points), n, int(merge_previous), _ptr(out),
+                                        _ptr(idx), _ptr(d8), dev))
+        return (out, idx, d8) if slots else out
+
+    # ---- quantities
+    def load_gaunt(self, table=None, x0=-6.0, y0=-16.0, dx=0.2, dy=0.2):
+        t = load_gaunt_table() if table is None else np.ascontiguousarray(table, np.float32)
+        self.check(self.L.ilc_gaunt_load(self.h, _ptr(t), t.shape[1], t.shape[0], x0, y0, dx, dy))
+        return t
+
+    def _q3(self, rho, u, xe):
+        dev = _is_dev(u)
+        if not dev:
+            rho = None if rho is None else np.ascontiguousarray(rho, np.float32)
+            u = np.ascontiguousarray(u, np.float32)
+            xe = np.ascontiguousarray(xe, np.float32)
+        n = u.shape[0]
+        if dev:
+            import torch
+            out = torch.empty(n, dtype=torch.float32, device=u.device)
+        else:
+            out = np.zeros(n, np.float32)
+        return rho, u, xe, n, out, dev
+
+    def xray_flux(self, rho, u, xe, redshift=REDSHIFT, luminosity_distance=LUMINOSITY_DISTANCE,
+                  e_min=0.1, e_max=10.0, num_samples=100):
+        rho, u, xe, n, out, dev = self._q3(rho, u, xe)
+        self.check(self.L.ilc_quantity_xray_flux(self.h, _ptr(rho), _ptr(u), _ptr(xe), n,
+                                                 redshift, luminosity_distance, e_min, e_max,
+                                                 num_samples, _ptr(out), dev))
+        return out
+
+    def xray_spectral_flux(self, rho, u, xe, energy, energy_bin_width, redshift=REDSHIFT,
+                           luminosity_distance=LUMINOSITY_DISTANCE):
+        rho, u, xe, n, out, dev = self._q3(rho, u, xe)
+        self.check(self.L.ilc_quantity_xray_spectral_flux(self.h, _ptr(rho), _ptr(u), _ptr(xe),
+                                                          n, redshift, luminosity_distance,
+                                                          energy, energy_bin_width, _ptr(out),
+                                                          dev))
+        return out
+
+    def mean_temperature(self, u, xe):
+        _, u, xe, n, out, dev = self._q3(None, u, xe)
+        self.check(self.L.ilc_quantity_temperature(self.h, _ptr(u), _ptr(xe), n, _ptr(out), dev))
+        return out
+
+    # ---- line of sight integration
+    def _image(self, cam, like_device):
+        if like_device:
+            import torch
+            return torch.empty((cam.num_pix_y, cam.num_pix_x), dtype=torch.float32,
+                               device=f"cuda:{self.device}")
+        return np.zeros((cam.num_pix_y, cam.num_pix_x), np.float32)
+
+    def render_adaptive(self, cam, z_range, rel_tol=1e-3, abs_tol=0.0,
+                        controller=CONTROLLER_FP64, scaling=None, device_output=False):
+        img = self._image(cam, device_output)
+        st = RenderStats()
+        sc = None if scaling is None else ctypes.byref(scaling)
+        self.check(self.L.ilc_render_adaptive(self.h, ctypes.byref(cam), float(z_range),
+                                              Tolerance(abs_tol, rel_tol), controller, sc,
+                                              _ptr(img), 1 if device_output else 0,
+                                              ctypes.byref(st)))
+        return img, st.as_dict()
+
+    def project_xray_flux(self, cells, rho, u, xe, cam, z_range, rel_tol=1e-3, abs_tol=0.0,
+                          controller=CONTROLLER_FP64, redshift=REDSHIFT,
+                          luminosity_distance=LUMINOSITY_DISTANCE, e_min=0.5, e_max=7.0,
+                          num_samples=100, scaling=None, image=None):
+        """X-ray band map from raw cells in one call (ilc_project_xray_flux).
+        Inputs are all host arrays or all device tensors; the image follows."""
+        dev = _is_dev(u)
+        if not dev:
+            cells = np.ascontiguousarray(cells, np.float32).reshape(-1, 4)
+            rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+        if image is None:
+            image = self._image(cam, dev)
+        st = RenderStats()
+        sc = None if scaling is None else ctypes.byref(scaling)
+        self.check(self.L.ilc_project_xray_flux(
+            self.h, _ptr(cells), _ptr(rho), _ptr(u), _ptr(xe), int(u.shape[0]), redshift,
+            luminosity_distance, e_min, e_max, num_samples, ctypes.byref(cam), float(z_range),
+            Tolerance(abs_tol, rel_tol), controller, sc, _ptr(image), dev, ctypes.byref(st)))
+        return image, st.as_dict()
+
+    @property
+    def kernel_launches(self):
+        return int(self.L.ilc_kernel_launches(self.h))
+
+    def render_fixed(self, cam, z_range, num_steps, scaling=None, device_output=False):
+        img = self._image(cam, device_output)
+        st = RenderStats()
+        sc = None if scaling is None else ctypes.byref(scaling)
+        self.check(self.L.ilc_render_fixed(self.h, ctypes.byref(cam), float(z_range),
+                                           int(num_steps), sc, _ptr(img),
+                                           1 if device_output else 0, ctypes.byref(st)))
+        return img, st.as_dict()
+
+
+class Nn8Backend:
+    """The reconstruction_backend interface (reconstruction_backend.hpp:35-58)
+    over the CUDA context; selectable as ``--reconstructor.voronoi nn8_cuda``."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self._points = None
+        self._first = True
+        self._result = None
+        self._blocksize = 0
+
+    def get_required_additional_datasets(self):
+        return []
+
+    def get_backend_name(self):
+        return "volumetric/nn8_cuda"
+
+    def init_backend(self, blocksize):
+        self._blocksize = int(blocksize)
+
+    def setup_particles(self, particles, additional_datasets=()):
+        self.ctx.setup_particles(particles)
+
+    def setup_evaluation_points(self, points, num_points=None):
+        pts = points if num_points is None else points[:num_points]
+        self._points = pts
+        self._first = True
+        self._result = None
+
+    def run(self):
+        if self._points is None:
+            raise IlcError(1, "run() before setup_evaluation_points()")
+        self._result = self.ctx.nn8_query(self._points, merge_previous=not self._first)
+        self._first = False
+
+    def retrieve_results(self):
+        return self._result
+
+
+def create_projection(ctx, cam, z_range, rel_tol=1e-2, abs_tol=0.0, dA_mode=DA_PIXEL_AREA,
+                      length_conversion=1.0, area_conversion=1.0, controller=CONTROLLER_FP64):
+    """volumetric_integration::create_projection: adaptive line-of-sight image,
+    scaled by length_conversion * dA_eff (volumetric_integration.cpp:74-87)."""
+    s = LosScaling(length_conversion, area_conversion, dA_mode)
+    return ctx.render_adaptive(cam, z_range, rel_tol, abs_tol, controller, scaling=s)

@@ -1,0 +1,556 @@
+// ilc_capi.cu -- the extern "C" boundary (include/ilc.h) over the CUDA path.
+//
+// Host-side arithmetic that the reference does on the CPU in double (grid
+// parameters, camera basis, image scaling) is done here the same way, so the
+// device receives the same float parameters the reference's kernels receive.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "ilc_internal.h"
+
+struct ilc_ctx {
+  ilc::Context c;
+};
+
+namespace ilc {
+namespace {
+
+ilc_status fail(Context& c, ilc_status st, const std::string& msg) {
+  c.error = msg;
+  return st;
+}
+
+ilc_status cuda_fail(Context& c, cudaError_t e, const char* where) {
+  const ilc_status st =
+      e == cudaErrorMemoryAllocation ? ILC_ERR_OUT_OF_MEMORY : ILC_ERR_CUDA;
+  c.error = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return st;
+}
+
+#define ILC_CUDA(ctx, expr, where)               \
+  do {                                           \
+    cudaError_t e_ = (expr);                     \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+  } while (0)
+
+// Stages a caller array on the device: returns the device pointer to use.
+cudaError_t stage_in(Context& c, DevBuf& buf, const void* src, size_t bytes, int is_device,
+                     const void** out) {
+  if (is_device) {
+    *out = src;
+    return cudaSuccess;
+  }
+  cudaError_t e = buf.ensure(bytes);
+  if (e) return e;
+  e = cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, c.stream);
+  *out = buf.p;
+  return e;
+}
+
+cudaError_t out_ptr(DevBuf& buf, void* dst, size_t bytes, int is_device, void** out) {
+  if (is_device) {
+    *out = dst;
+    return cudaSuccess;
+  }
+  cudaError_t e = buf.ensure(bytes);
+  *out = buf.p;
+  return e;
+}
+
+cudaError_t finish_out(Context& c, void* dst, const void* dev, size_t bytes, int is_device) {
+  if (!is_device && bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, c.stream);
+    if (e) return e;
+  }
+  return cudaStreamSynchronize(c.stream);
+}
+
+// particle_grid ctor (particle_grid.cpp:54-103): bounding box +-0.1 in double,
+// cell width cbrt(8/N * V), n_cells = ceil(extent / width), float casts.
+void make_grid_params(const float mn_f[3], const float mx_f[3], uint64_t n, GridParams* g) {
+  double mn[3], mx[3];
+  for (int i = 0; i < 3; ++i) { mn[i] = (double)mn_f[i]; mx[i] = (double)mx_f[i]; }
+  double vol = 1.0;
+  for (int i = 0; i < 3; ++i) {
+    mn[i] -= 0.1;
+    mx[i] += 0.1;
+    vol *= (mx[i] - mn[i]);
+  }
+  const double cell_volume = (double)8 / (double)n * vol;
+  const double w = std::cbrt(cell_volume);
+  g->total = 1;
+  for (int i = 0; i < 3; ++i) {
+    g->n[i] = (int32_t)std::ceil((mx[i] - mn[i]) / w);
+    g->min[i] = (float)mn[i];
+    g->cs[i] = (float)w;
+    g->total *= (uint64_t)g->n[i];
+  }
+}
+
+// camera::update_basis_vectors / update_min_position (camera.cpp:124-155,
+// math.hpp:85-149), in double, then cast to float.
+void camera_plane(const ilc_camera& cam, float out[13]) {
+  auto dot3 = [](const double* a, const double* b) {
+    double r = 0.0;
+    for (int i = 0; i < 3; ++i) r += a[i] * b[i];
+    return r;
+  };
+  auto cross3 = [](const double* a, const double* b, double* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  const double ps = cam.screen_width / (double)cam.num_pix_x;
+  double v1[3] = {0, 0, 1};
+  if (cam.look_at[0] == v1[0] && cam.look_at[1] == v1[1] && cam.look_at[2] == v1[2]) {
+    v1[0] = 0; v1[1] = 1; v1[2] = 0;
+  }
+  double a[3], b[3];
+  cross3(v1, cam.look_at, a);
+  cross3(cam.look_at, a, b);
+  const double a1 = cam.look_at[0], a2 = cam.look_at[1], a3 = cam.look_at[2];
+  const double a1a2 = a1 * a2, a1a3 = a1 * a3, a2a3 = a2 * a3;
+  const double ca = std::cos(cam.roll), sa = std::sin(cam.roll);
+  const double fc = 1.0 - ca;
+  const double m[3][3] = {{a1 * a1 * fc + ca, a1a2 * fc - a3 * sa, a1a3 * fc + a2 * sa},
+                          {a1a2 * fc + a3 * sa, a2 * a2 * fc + ca, a2a3 * fc - a1 * sa},
+                          {a1a3 * fc - a2 * sa, a2a3 * fc + a1 * sa, a3 * a3 * fc + ca}};
+  double ra[3], rb[3];
+  for (int i = 0; i < 3; ++i) { ra[i] = dot3(m[i], a); rb[i] = dot3(m[i], b); }
+  const double la = 1. / std::sqrt(dot3(ra, ra)), lb = 1. / std::sqrt(dot3(rb, rb));
+  double b0[3], b1[3], mp[3];
+  for (int i = 0; i < 3; ++i) { b0[i] = la * ra[i]; b1[i] = lb * rb[i]; }
+  for (int i = 0; i < 3; ++i) mp[i] = cam.position[i];
+  for (int i = 0; i < 3; ++i) mp[i] -= ((double)cam.num_pix_x / 2.0) * ps * b0[i];
+  for (int i = 0; i < 3; ++i) mp[i] -= ((double)cam.num_pix_y / 2.0) * ps * b1[i];
+  for (int i = 0; i < 3; ++i) {
+    out[i] = (float)cam.look_at[i];
+    out[3 + i] = (float)b0[i];
+    out[6 + i] = (float)b1[i];
+    out[9 + i] = (float)mp[i];
+  }
+  out[12] = (float)ps;
+}
+
+float los_scale(const ilc_camera& cam, double z_range, const ilc_los_scaling& s) {
+  const double ps = cam.screen_width / (double)cam.num_pix_x;
+  const float pixel_area = (float)(ps * ps);
+  const float lc = (float)s.length_conversion;
+  const double dA_in = (double)pixel_area * s.area_conversion;
+  const double range = (double)lc * z_range;
+  double dA;
+  if (s.dA_mode == ILC_DA_PIXEL_AREA) dA = dA_in;
+  else if (s.dA_mode == ILC_DA_UNIT) dA = 1.0;
+  else dA = 1.0 / range;
+  const float dAf = (float)dA;
+  return lc * dAf;
+}
+
+bool camera_ok(const ilc_camera* cam) {
+  if (!cam || cam->num_pix_x <= 0 || cam->num_pix_y <= 0) return false;
+  if (!(cam->screen_width > 0.0)) return false;
+  const double l2 = cam->look_at[0] * cam->look_at[0] + cam->look_at[1] * cam->look_at[1] +
+                    cam->look_at[2] * cam->look_at[2];
+  return l2 > 0.0 && std::isfinite(l2);
+}
+
+ilc_status read_flags(Context& c, uint32_t* flags, DevStats* stats) {
+  char buf[kFlagsBytes];
+  ILC_CUDA(c, cudaMemcpyAsync(buf, c.flags.p, kFlagsBytes, cudaMemcpyDeviceToHost, c.stream),
+           "read flags");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "read flags");
+  std::memcpy(flags, buf, 4);
+  if (stats) std::memcpy(stats, buf + 64, sizeof(DevStats));
+  return ILC_OK;
+}
+
+ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_tolerance tol,
+                         int32_t controller, int64_t fixed_steps,
+                         const ilc_los_scaling* scaling, float* image, int is_device,
+                         ilc_render_stats* stats) {
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "render before setup_particles");
+  if (!camera_ok(cam)) return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid camera");
+  if (!(z_range > 0.0) || !std::isfinite(z_range) || !image)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z_range or image");
+  if (fixed_steps <= 0) {
+    if (!(tol.absolute >= 0.0) || !(tol.relative >= 0.0) ||
+        (tol.absolute <= 0.0 && tol.relative <= 0.0))
+      return fail(c, ILC_ERR_INVALID_ARGUMENT,
+                  "either the absolute or the relative tolerance has to be > 0");
+    if (controller != ILC_CONTROLLER_REF32 && controller != ILC_CONTROLLER_FP64)
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "unknown controller");
+  }
+  RenderArgs a{};
+  camera_plane(*cam, a.cam);
+  a.nx = cam->num_pix_x;
+  a.ny = cam->num_pix_y;
+  a.z0 = 0.0f;
+  a.z_end = (float)z_range;
+  a.atol = tol.absolute;
+  a.rtol = tol.relative;
+  a.controller = controller;
+  a.fixed_steps = fixed_steps;
+  a.fixed_h = fixed_steps > 0 ? (float)(z_range / (double)fixed_steps) : 0.0f;
+  a.apply_scale = scaling != nullptr;
+  a.scale = scaling ? los_scale(*cam, z_range, *scaling) : 1.0f;
+  const size_t bytes = (size_t)a.nx * (size_t)a.ny * 4;
+  void* dimg = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, image, bytes, is_device, &dimg), "image buffer");
+  a.out = static_cast<float*>(dimg);
+  float ms = 0.0f;
+  ILC_CUDA(c, render_launch(c, a, &ms), "render kernel");
+  ILC_CUDA(c, finish_out(c, image, dimg, bytes, is_device), "render");
+  uint32_t flags = 0;
+  DevStats ds{};
+  ilc_status st = read_flags(c, &flags, &ds);
+  if (st) return st;
+  if (stats) {
+    stats->steps = ds.steps;
+    stats->accepted_steps = ds.accepted;
+    stats->queries = ds.queries;
+    stats->cells_visited = ds.cells;
+    stats->candidates = ds.cands;
+    stats->max_steps_per_ray = ds.max_steps;
+    stats->rays_at_step_limit = ds.rays_at_limit;
+    stats->kernel_ms = ms;
+  }
+  if (flags & FLAG_STEP_LIMIT)
+    return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the per-ray step limit");
+  return ILC_OK;
+}
+
+}  // namespace
+}  // namespace ilc
+
+using namespace ilc;
+
+extern "C" {
+
+ilc_ctx* ilc_create(int device) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+  ilc_ctx* h = new (std::nothrow) ilc_ctx();
+  if (!h) return nullptr;
+  Context& c = h->c;
+  c.device = device;
+  if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return nullptr;
+  }
+  c.own_stream = true;
+  int8_t t[8][125][3];
+  spiral_table(t);
+  char4 packed[1000];
+  for (int s = 0; s < 8; ++s)
+    for (int i = 0; i < 125; ++i)
+      packed[s * 125 + i] = make_char4(t[s][i][0], t[s][i][1], t[s][i][2], 0);
+  if (c.spiral.ensure(sizeof(packed)) ||
+      cudaMemcpy(c.spiral.p, packed, sizeof(packed), cudaMemcpyHostToDevice) ||
+      c.flags.ensure(kFlagsBytes)) {
+    ilc_destroy(h);
+    return nullptr;
+  }
+  return h;
+}
+
+void ilc_destroy(ilc_ctx* h) {
+  if (!h) return;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  for (DevBuf* b : {&c.parts, &c.cells, &c.s2u, &c.keys_a, &c.keys_b, &c.vals_a, &c.vals_b,
+                    &c.hist, &c.tmp_in, &c.gaunt, &c.list_d, &c.list_v, &c.list_id, &c.in_a,
+                    &c.in_b, &c.in_c, &c.out_a, &c.out_b, &c.out_c, &c.spiral, &c.flags})
+    b->release();
+  if (c.ev0) cudaEventDestroy(c.ev0);
+  if (c.ev1) cudaEventDestroy(c.ev1);
+  if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+  delete h;
+}
+
+const char* ilc_last_error(const ilc_ctx* h) { return h ? h->c.error.c_str() : "null context"; }
+
+ilc_status ilc_set_step_limit(ilc_ctx* h, int64_t max_steps) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  if (max_steps <= 0) return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "step limit must be > 0");
+  h->c.max_steps = max_steps;
+  return ILC_OK;
+}
+
+void* ilc_get_stream(ilc_ctx* h) { return h ? (void*)h->c.stream : nullptr; }
+
+ilc_status ilc_nn8_setup_particles(ilc_ctx* h, const float* particles, uint64_t n,
+                                   int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!particles || n == 0) return fail(c, ILC_ERR_INVALID_ARGUMENT, "no particles");
+  if (n >= (1ull << 31)) return fail(c, ILC_ERR_GRID_TOO_LARGE, "more than 2^31 particles");
+  c.has_grid = false;
+  const void* din = nullptr;
+  ILC_CUDA(c, stage_in(c, c.tmp_in, particles, n * 16, is_device, &din), "particles H2D");
+  float mn[3], mx[3];
+  bool nonfinite = false;
+  ILC_CUDA(c, grid_bbox(c, static_cast<const float4*>(din), n, mn, mx, &nonfinite),
+           "bounding box");
+  if (nonfinite) return fail(c, ILC_ERR_NONFINITE_INPUT, "non-finite particle coordinates");
+  GridParams g;
+  make_grid_params(mn, mx, n, &g);
+  if (g.total >= (1ull << 32) || g.n[0] <= 0 || g.n[1] <= 0 || g.n[2] <= 0)
+    return fail(c, ILC_ERR_GRID_TOO_LARGE, "grid has more than 2^32 cells");
+  c.gp = g;
+  ILC_CUDA(c, grid_build_device(c, static_cast<const float4*>(din), n), "grid build");
+  uint32_t flags = 0;
+  ilc_status st = read_flags(c, &flags, nullptr);
+  if (st) return st;
+  if (flags & FLAG_KEY_RANGE) return fail(c, ILC_ERR_INTERNAL, "particle outside its grid");
+  c.n_particles = n;
+  c.has_grid = true;
+  c.list_n = 0;
+  return ILC_OK;
+}
+
+ilc_status ilc_grid_describe(ilc_ctx* h, ilc_grid_desc* out) {
+  if (!h || !out) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "no grid");
+  for (int i = 0; i < 3; ++i) {
+    out->min_corner[i] = c.gp.min[i];
+    out->cell_sizes[i] = c.gp.cs[i];
+    out->num_cells[i] = c.gp.n[i];
+  }
+  out->total_cells = c.gp.total;
+  out->num_particles = c.n_particles;
+  return ILC_OK;
+}
+
+ilc_status ilc_grid_export(ilc_ctx* h, int32_t* cells, uint32_t* s2u, float* sorted,
+                           int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "no grid");
+  const cudaMemcpyKind k = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (cells)
+    ILC_CUDA(c, cudaMemcpyAsync(cells, c.cells.p, c.gp.total * 8, k, c.stream), "export cells");
+  if (s2u)
+    ILC_CUDA(c, cudaMemcpyAsync(s2u, c.s2u.p, c.n_particles * 4, k, c.stream), "export s2u");
+  if (sorted)
+    ILC_CUDA(c, cudaMemcpyAsync(sorted, c.parts.p, c.n_particles * 16, k, c.stream),
+             "export particles");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "export");
+  return ILC_OK;
+}
+
+ilc_status ilc_nn8_query(ilc_ctx* h, const float* points, uint64_t n, int merge_previous,
+                         float* out_values, int32_t* out_idx8, float* out_dist8,
+                         int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "query before setup_particles");
+  if (n == 0) return ILC_OK;
+  if (!points || !out_values) return fail(c, ILC_ERR_INVALID_ARGUMENT, "null array");
+  if (merge_previous && c.list_n != n)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "merge_previous needs the same point count");
+  const void* dp = nullptr;
+  void *dv = nullptr, *di = nullptr, *dd = nullptr;
+  ILC_CUDA(c, stage_in(c, c.in_a, points, n * 16, is_device, &dp), "points H2D");
+  ILC_CUDA(c, out_ptr(c.out_a, out_values, n * 4, is_device, &dv), "values");
+  if (out_idx8) ILC_CUDA(c, out_ptr(c.out_b, out_idx8, n * 32, is_device, &di), "idx");
+  if (out_dist8) ILC_CUDA(c, out_ptr(c.out_c, out_dist8, n * 32, is_device, &dd), "dist");
+  ILC_CUDA(c, nn8_query_launch(c, static_cast<const float4*>(dp), n, merge_previous != 0,
+                               static_cast<float*>(dv), static_cast<int32_t*>(di),
+                               static_cast<float*>(dd)),
+           "nn8 kernel");
+  if (!is_device) {
+    ILC_CUDA(c, cudaMemcpyAsync(out_values, dv, n * 4, cudaMemcpyDeviceToHost, c.stream), "D2H");
+    if (out_idx8)
+      ILC_CUDA(c, cudaMemcpyAsync(out_idx8, di, n * 32, cudaMemcpyDeviceToHost, c.stream), "D2H");
+    if (out_dist8)
+      ILC_CUDA(c, cudaMemcpyAsync(out_dist8, dd, n * 32, cudaMemcpyDeviceToHost, c.stream), "D2H");
+  }
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "nn8 query");
+  return ILC_OK;
+}
+
+ilc_status ilc_gaunt_load(ilc_ctx* h, const float* table, int32_t width, int32_t height,
+                          float x0, float y0, float dx, float dy) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!table || width <= 0 || height <= 0 || width * height > 81 * 146 || !(dx > 0.0f) ||
+      !(dy > 0.0f))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid Gaunt table (at most 81 x 146 entries)");
+  const size_t bytes = (size_t)width * height * 4;
+  ILC_CUDA(c, c.gaunt.ensure(bytes), "gaunt alloc");
+  ILC_CUDA(c, cudaMemcpyAsync(c.gaunt.p, table, bytes, cudaMemcpyHostToDevice, c.stream),
+           "gaunt H2D");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "gaunt");
+  c.gw = width; c.gh = height; c.gx0 = x0; c.gy0 = y0; c.gdx = dx; c.gdy = dy;
+  c.has_gaunt = true;
+  return ILC_OK;
+}
+
+static ilc_status quantity_inputs(Context& c, const float* rho, const float* u, const float* xe,
+                                  uint64_t n, int is_device, const float** drho,
+                                  const float** du, const float** dxe) {
+  const void *a = nullptr, *b = nullptr, *d = nullptr;
+  if (rho) ILC_CUDA(c, stage_in(c, c.in_a, rho, n * 4, is_device, &a), "rho H2D");
+  if (u) ILC_CUDA(c, stage_in(c, c.in_b, u, n * 4, is_device, &b), "u H2D");
+  if (xe) ILC_CUDA(c, stage_in(c, c.in_c, xe, n * 4, is_device, &d), "xe H2D");
+  *drho = static_cast<const float*>(a);
+  *du = static_cast<const float*>(b);
+  *dxe = static_cast<const float*>(d);
+  return ILC_OK;
+}
+
+ilc_status ilc_quantity_xray_flux(ilc_ctx* h, const float* rho, const float* u, const float* xe,
+                                  uint64_t n, float redshift, float luminosity_distance,
+                                  float e_min, float e_max, int32_t num_samples, float* out,
+                                  int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (n == 0) return ILC_OK;
+  if (!rho || !u || !xe || !out || num_samples <= 0 || !(e_max >= e_min))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid xray_flux arguments");
+  const float *a, *b, *d;
+  ilc_status st = quantity_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  void* dout = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, out, n * 4, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_xray_flux_launch(c, a, b, d, n, redshift, luminosity_distance, e_min,
+                                        e_max, num_samples, static_cast<float*>(dout)),
+           "xray_flux kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, n * 4, is_device), "xray_flux");
+  return ILC_OK;
+}
+
+ilc_status ilc_quantity_xray_spectral_flux(ilc_ctx* h, const float* rho, const float* u,
+                                           const float* xe, uint64_t n, float redshift,
+                                           float luminosity_distance, float energy,
+                                           float energy_bin_width, float* out, int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (n == 0) return ILC_OK;
+  if (!rho || !u || !xe || !out)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid xray_spectral_flux arguments");
+  const float *a, *b, *d;
+  ilc_status st = quantity_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  void* dout = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, out, n * 4, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_xray_bin_launch(c, a, b, d, n, redshift, luminosity_distance, energy,
+                                       energy_bin_width, static_cast<float*>(dout)),
+           "xray_spectral_flux kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, n * 4, is_device), "xray_spectral_flux");
+  return ILC_OK;
+}
+
+ilc_status ilc_quantity_temperature(ilc_ctx* h, const float* u, const float* xe, uint64_t n,
+                                    float* out, int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (n == 0) return ILC_OK;
+  if (!u || !xe || !out) return fail(c, ILC_ERR_INVALID_ARGUMENT, "null array");
+  const float *a, *b, *d;
+  ilc_status st = quantity_inputs(c, nullptr, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  void* dout = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, out, n * 4, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_temperature_launch(c, b, d, n, static_cast<float*>(dout)),
+           "temperature kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, n * 4, is_device), "temperature");
+  return ILC_OK;
+}
+
+ilc_status ilc_camera_plane(const ilc_camera* cam, float* out13) {
+  if (!camera_ok(cam) || !out13) return ILC_ERR_INVALID_ARGUMENT;
+  camera_plane(*cam, out13);
+  return ILC_OK;
+}
+
+ilc_status ilc_render_adaptive(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                               ilc_tolerance tol, int32_t controller,
+                               const ilc_los_scaling* scaling, float* image, int is_device,
+                               ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(h->c.device);
+  return render_common(h->c, cam, z_range, tol, controller, 0, scaling, image, is_device, stats);
+}
+
+ilc_status ilc_render_fixed(ilc_ctx* h, const ilc_camera* cam, double z_range, int64_t num_steps,
+                            const ilc_los_scaling* scaling, float* image, int is_device,
+                            ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(h->c.device);
+  if (num_steps <= 0) return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "num_steps must be > 0");
+  return render_common(h->c, cam, z_range, ilc_tolerance{0.0, 0.0}, ILC_CONTROLLER_REF32,
+                       num_steps, scaling, image, is_device, stats);
+}
+
+float ilc_los_scale(const ilc_camera* cam, double z_range, const ilc_los_scaling* scaling) {
+  if (!camera_ok(cam) || !scaling) return 0.0f;
+  return los_scale(*cam, z_range, *scaling);
+}
+
+ilc_status ilc_project_xray_flux(ilc_ctx* h, const float* cells, const float* rho,
+                                 const float* u, const float* xe, uint64_t n, float redshift,
+                                 float luminosity_distance, float e_min, float e_max,
+                                 int32_t num_samples, const ilc_camera* cam, double z_range,
+                                 ilc_tolerance tol, int32_t controller,
+                                 const ilc_los_scaling* scaling, float* image, int is_device,
+                                 ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (!cells || !rho || !u || !xe || n == 0 || num_samples <= 0 || !(e_max >= e_min))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid band-map arguments");
+  if (n >= (1ull << 31)) return fail(c, ILC_ERR_GRID_TOO_LARGE, "more than 2^31 particles");
+  // Particle records are assembled in the context's staging buffer, whose q
+  // slot the quantity kernel fills (stride 4) -- the crawler's packing step.
+  ILC_CUDA(c, c.tmp_in.ensure(n * 16), "particle staging");
+  ILC_CUDA(c, cudaMemcpyAsync(c.tmp_in.p, cells, n * 16,
+                              is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                              c.stream),
+           "cells copy");
+  const float *a, *b, *d;
+  ilc_status st = quantity_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  ILC_CUDA(c, quantity_xray_flux_launch(c, a, b, d, n, redshift, luminosity_distance, e_min,
+                                        e_max, num_samples, c.tmp_in.as<float>() + 3, 4),
+           "xray_flux kernel");
+  c.has_grid = false;
+  float mn[3], mx[3];
+  bool nonfinite = false;
+  ILC_CUDA(c, grid_bbox(c, c.tmp_in.as<float4>(), n, mn, mx, &nonfinite), "bounding box");
+  if (nonfinite) return fail(c, ILC_ERR_NONFINITE_INPUT, "non-finite particle coordinates");
+  GridParams g;
+  make_grid_params(mn, mx, n, &g);
+  if (g.total >= (1ull << 32) || g.n[0] <= 0 || g.n[1] <= 0 || g.n[2] <= 0)
+    return fail(c, ILC_ERR_GRID_TOO_LARGE, "grid has more than 2^32 cells");
+  c.gp = g;
+  ILC_CUDA(c, grid_build_device(c, c.tmp_in.as<float4>(), n), "grid build");
+  uint32_t flags = 0;
+  st = read_flags(c, &flags, nullptr);
+  if (st) return st;
+  if (flags & FLAG_KEY_RANGE) return fail(c, ILC_ERR_INTERNAL, "particle outside its grid");
+  c.n_particles = n;
+  c.has_grid = true;
+  c.list_n = 0;
+  return render_common(c, cam, z_range, tol, controller, 0, scaling, image, is_device, stats);
+}
+
+uint64_t ilc_kernel_launches(const ilc_ctx* h) { return h ? h->c.launches : 0; }
+
+}  // extern "C"

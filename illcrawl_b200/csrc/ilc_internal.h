@@ -1,0 +1,134 @@
+// ilc_internal.h -- host-side state shared by the CUDA translation units and the
+// C ABI: the context (stream, device buffers, last error) and kernel launchers.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ilc.h"
+
+namespace ilc {
+
+// Grow-only device buffer: reallocated only when a call needs more room, so a
+// render loop does not allocate per call (the reference reallocates its nn8
+// list buffers on every setup_evaluation_points).
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Host copy of the particle grid parameters (particle_grid.cpp:54-103).
+struct GridParams {
+  float min[3];
+  float cs[3];
+  int32_t n[3];
+  uint64_t total;
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string error;
+  int64_t max_steps = 1 << 20;  // per-ray RKF step cap
+
+  // particle grid
+  bool has_grid = false;
+  uint64_t n_particles = 0;
+  GridParams gp{};
+  DevBuf parts;      // float4 sorted particles
+  DevBuf cells;      // int2 per grid cell
+  DevBuf s2u;        // uint32 sorted -> original index
+  DevBuf keys_a, keys_b, vals_a, vals_b, hist, tmp_in;  // build scratch
+
+  // Gaunt table
+  bool has_gaunt = false;
+  DevBuf gaunt;
+  int32_t gw = 0, gh = 0;
+  float gx0 = 0, gy0 = 0, gdx = 0, gdy = 0;
+
+  // nn8 running lists for multi-block merging (volumetric_reconstruction_backend_nn8.cpp:57-66)
+  DevBuf list_d, list_v, list_id;
+  uint64_t list_n = 0;
+
+  // generic per-call staging
+  DevBuf in_a, in_b, in_c, out_a, out_b, out_c;
+  DevBuf spiral;     // char4[1000]
+  DevBuf flags;      // uint32 error flags + uint64 stats
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint64_t launches = 0;  // kernels this context has launched
+};
+
+// Error flags written by kernels (bit mask in flags[0]).
+enum : uint32_t {
+  FLAG_KEY_RANGE = 1u,
+  FLAG_STEP_LIMIT = 2u,
+  FLAG_NONFINITE = 4u,
+};
+
+// Stats block layout behind the flags word (uint64 counters).
+struct DevStats {
+  unsigned long long steps;
+  unsigned long long accepted;
+  unsigned long long queries;
+  unsigned long long cells;
+  unsigned long long cands;
+  unsigned long long max_steps;
+  unsigned long long rays_at_limit;
+  unsigned long long pad;
+};
+constexpr size_t kFlagsBytes = 64 + sizeof(DevStats);
+
+// launchers (return cudaError_t of the launch sequence)
+cudaError_t grid_bbox(Context& c, const float4* in, uint64_t n, float* mn3, float* mx3,
+                      bool* nonfinite);
+cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n);
+cudaError_t nn8_query_launch(Context& c, const float4* pts, uint64_t n, bool merge,
+                             float* out, int32_t* idx8, float* d8);
+cudaError_t quantity_xray_flux_launch(Context& c, const float* rho, const float* u,
+                                      const float* xe, uint64_t n, float z, float dL,
+                                      float emin, float emax, int num_samples, float* out,
+                                      int out_stride = 1);
+cudaError_t quantity_xray_bin_launch(Context& c, const float* rho, const float* u,
+                                     const float* xe, uint64_t n, float z, float dL, float e,
+                                     float de, float* out);
+cudaError_t quantity_temperature_launch(Context& c, const float* u, const float* xe,
+                                        uint64_t n, float* out);
+
+struct RenderArgs {
+  float cam[13];        // look(3), b0(3), b1(3), min corner(3), pixel size
+  int32_t nx, ny;
+  float z0, z_end;
+  double atol, rtol;
+  int32_t controller;   // ILC_CONTROLLER_*
+  int64_t fixed_steps;  // > 0: fixed-step mode
+  float fixed_h;        // step of the fixed-step mode, (float)(z_range / fixed_steps)
+  float scale;          // multiplier applied to each pixel
+  bool apply_scale;
+  float* out;           // device image
+};
+cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms);
+
+// Spiral table (8 subcells x 125 offsets), generated on the host.
+void spiral_table(int8_t out[8][125][3]);
+
+}  // namespace ilc

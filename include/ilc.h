@@ -1,0 +1,219 @@
+/* ilc.h -- C ABI of the B200 (sm_100a) backend for illcrawl's volumetric
+ * projection path: nn8 particle-grid reconstruction feeding the RKF4(5)
+ * line-of-sight integrator that produces gas projections, X-ray band maps and
+ * X-ray spectra.
+ *
+ * Conventions
+ *  - Every call returns an ilc_status; ILC_OK is 0. The message of the last
+ *    failure on a context is returned by ilc_last_error().
+ *  - A context owns one CUDA stream, the device copy of the particle grid, the
+ *    Gaunt table and grow-only scratch buffers. Calls on one context must be
+ *    serialised by the caller (one context per host thread); every call has
+ *    completed on the device when it returns.
+ *  - Arrays are caller-allocated. is_device = 0: host pointers (copied in and
+ *    out by the call); is_device = 1: device pointers on the context's device.
+ *  - Particles are float4 records (x, y, z, q) -- the reference's particle
+ *    layout (particle_grid.hpp:43-48).
+ *  - Nothing here falls back to the CPU: without a usable CUDA device
+ *    ilc_create() returns NULL.
+ */
+#ifndef ILC_H
+#define ILC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ilc_status {
+  ILC_OK = 0,
+  ILC_ERR_INVALID_ARGUMENT = 1,
+  ILC_ERR_CUDA = 2,
+  ILC_ERR_OUT_OF_MEMORY = 3,
+  ILC_ERR_NO_PARTICLES = 4,    /* query or render before setup_particles */
+  ILC_ERR_NO_GAUNT_TABLE = 5,  /* X-ray quantity before ilc_gaunt_load */
+  ILC_ERR_STEP_LIMIT = 6,      /* a ray reached the per-ray RKF step cap */
+  ILC_ERR_NONFINITE_INPUT = 7, /* NaN or Inf particle coordinates */
+  ILC_ERR_GRID_TOO_LARGE = 8,  /* more than 2^32 grid cells or 2^31 particles */
+  ILC_ERR_INTERNAL = 9
+} ilc_status;
+
+typedef struct ilc_ctx ilc_ctx;
+
+/* camera (camera.hpp:493-593): position of the screen centre, normalised
+ * look-at direction, roll angle [rad], screen width, resolution. */
+typedef struct ilc_camera {
+  double position[3];
+  double look_at[3];
+  double roll;
+  double screen_width;
+  int32_t num_pix_x;
+  int32_t num_pix_y;
+} ilc_camera;
+
+/* integration::tolerance (integration.hpp:37-49) */
+typedef struct ilc_tolerance {
+  double absolute;
+  double relative;
+} ilc_tolerance;
+
+/* Step controller of the adaptive integrator. REF32: the reference's fp32
+ * controller (integration.cl:49-131). FP64: the same controller evaluated in
+ * double over the fp32 state. */
+enum { ILC_CONTROLLER_REF32 = 0, ILC_CONTROLLER_FP64 = 1 };
+
+/* effective_line_of_sight_integration_dA of the reconstructed quantity
+ * (quantity.hpp:56-57): PIXEL_AREA for fluxes (quantity.hpp:198-202), UNIT for
+ * projected density (quantity.hpp:567-572), INVERSE_RANGE for mean
+ * quantities (quantity.hpp:482-487). */
+enum { ILC_DA_PIXEL_AREA = 0, ILC_DA_UNIT = 1, ILC_DA_INVERSE_RANGE = 2 };
+
+/* Final image scaling of volumetric_integration.cpp:74-87. */
+typedef struct ilc_los_scaling {
+  double length_conversion; /* unit_converter::length_conversion_factor() */
+  double area_conversion;   /* unit_converter::area_conversion_factor() */
+  int32_t dA_mode;          /* ILC_DA_* */
+} ilc_los_scaling;
+
+typedef struct ilc_grid_desc {
+  float min_corner[3];
+  float cell_sizes[3];
+  int32_t num_cells[3];
+  uint64_t total_cells;
+  uint64_t num_particles;
+} ilc_grid_desc;
+
+typedef struct ilc_render_stats {
+  uint64_t steps;          /* RKF steps over all rays (accepted + rejected) */
+  uint64_t accepted_steps;
+  uint64_t queries;        /* nn8 evaluations (4 per step) */
+  uint64_t cells_visited;  /* in-grid cells walked by all queries */
+  uint64_t candidates;     /* particles tested by all queries */
+  uint64_t max_steps_per_ray;
+  uint64_t rays_at_step_limit;
+  float kernel_ms;         /* device time of the render kernel (CUDA events) */
+} ilc_render_stats;
+
+/* ---- context (replaces qcl::device_context, qcl.hpp:196-890, for this path) */
+ilc_ctx* ilc_create(int device);
+void ilc_destroy(ilc_ctx* ctx);
+const char* ilc_last_error(const ilc_ctx* ctx);
+/* Per-ray RKF step cap (default 2^20); reaching it ends the ray and makes the
+ * render return ILC_ERR_STEP_LIMIT. */
+ilc_status ilc_set_step_limit(ilc_ctx* ctx, int64_t max_steps);
+/* The context's cudaStream_t, for callers that time or order work around it. */
+void* ilc_get_stream(ilc_ctx* ctx);
+
+/* ---- particle grid + nn8 backend ------------------------------------------
+ * ilc_nn8_setup_particles replaces reconstruction_backend::setup_particles
+ * (reconstruction_backend.hpp:49-50) as implemented by nn8::setup_particles
+ * (volumetric_reconstruction_backend_nn8.cpp:47-55), which builds a
+ * particle_grid (particle_grid.cpp:25-119): grid over the particles' bounding
+ * box +-0.1, cell width cbrt(8 V / N), cells sorted by key. */
+ilc_status ilc_nn8_setup_particles(ilc_ctx* ctx, const float* particles, uint64_t n,
+                                   int is_device);
+
+/* particle_grid::get_grid_min_corner / get_num_grid_cells /
+ * get_grid_cell_sizes / get_num_particles (particle_grid.hpp:62-77). */
+ilc_status ilc_grid_describe(ilc_ctx* ctx, ilc_grid_desc* out);
+
+/* Copies the grid out: cells (int2 [begin, end) per cell, total_cells x 2),
+ * sorted->original index map (uint32, n) and sorted particles (float4, n).
+ * Any pointer may be NULL. particle_grid::get_grid_cells_buffer /
+ * get_particle_buffer and generate_sorted_to_unsorted_map
+ * (particle_grid.hpp:68-70,102-103). */
+ilc_status ilc_grid_export(ilc_ctx* ctx, int32_t* cells, uint32_t* sorted_to_unsorted,
+                           float* sorted_particles, int is_device);
+
+/* nn8 reconstruction at n query points (float4, w ignored). Replaces
+ * setup_evaluation_points + run + retrieve_results
+ * (reconstruction_backend.hpp:43,52-55; volumetric_reconstruction_backend_nn8.cpp:57-84).
+ * merge_previous = 0 starts from empty lists (is_first_run); 1 continues the
+ * lists the previous call on this context left for the same n, which is how
+ * the reference merges particle blocks. out_values: n floats. out_idx8 /
+ * out_dist8 (n x 8, may be NULL): the 8 list slots in slot order as original
+ * particle indices (-1 = empty) and distances. */
+ilc_status ilc_nn8_query(ilc_ctx* ctx, const float* points, uint64_t n, int merge_previous,
+                         float* out_values, int32_t* out_idx8, float* out_dist8,
+                         int is_device);
+
+/* ---- quantities ------------------------------------------------------------
+ * Thermally averaged free-free Gaunt factors, width x height row-major (row =
+ * one log(u), column = one log(gamma^2)), origin (x0, y0), spacing (dx, dy):
+ * model::gaunt::thermally_averaged_ff (gaunt_factor.cpp:30-41; the reference
+ * loads gaunt_factor.dat with x0 = -6, y0 = -16, dx = dy = 0.2). At most
+ * 81 x 146 entries. */
+ilc_status ilc_gaunt_load(ilc_ctx* ctx, const float* table, int32_t width, int32_t height,
+                          float x0, float y0, float dx, float dy);
+
+/* Per-cell band flux [keV/s/kpc^3/m^2]: the xray_flux kernel
+ * (quantities.cl:354-385) run by quantity_transformation (quantity.cpp:111-131).
+ * rho [M_sun/kpc^3], u [(km/s)^2], xe: n floats each. */
+ilc_status ilc_quantity_xray_flux(ilc_ctx* ctx, const float* rho, const float* u,
+                                  const float* xe, uint64_t n, float redshift,
+                                  float luminosity_distance, float e_min, float e_max,
+                                  int32_t num_samples, float* out, int is_device);
+
+/* Per-cell flux in one energy bin: xray_spectral_flux (quantities.cl:400-430). */
+ilc_status ilc_quantity_xray_spectral_flux(ilc_ctx* ctx, const float* rho, const float* u,
+                                           const float* xe, uint64_t n, float redshift,
+                                           float luminosity_distance, float energy,
+                                           float energy_bin_width, float* out,
+                                           int is_device);
+
+/* Per-cell temperature [K]: mean_temperature (quantities.cl:268-284). */
+ilc_status ilc_quantity_temperature(ilc_ctx* ctx, const float* u, const float* xe, uint64_t n,
+                                    float* out, int is_device);
+
+/* ---- camera and line-of-sight integration -----------------------------------
+ * The camera plane as the device sees it (camera.cpp:124-155 in double, cast
+ * to float as math::to_device_vector4): out13 = look_at(3), basis0(3),
+ * basis1(3), screen min corner(3), pixel size. */
+ilc_status ilc_camera_plane(const ilc_camera* cam, float* out13);
+
+/* volumetric_integration::create_projection (volumetric_integration.cpp:32-88):
+ * one adaptive RKF4(5) integrator per pixel from z = 0 to z_range along
+ * look_at, integrand = nn8 reconstruction of the particles' q. image:
+ * num_pix_y x num_pix_x floats (row = y). scaling = NULL leaves the raw line
+ * integrals; otherwise they are multiplied as volumetric_integration.cpp:74-87.
+ * stats may be NULL. */
+ilc_status ilc_render_adaptive(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                               ilc_tolerance tol, int32_t controller,
+                               const ilc_los_scaling* scaling, float* image, int is_device,
+                               ilc_render_stats* stats);
+
+/* Frozen uniform step sequence: num_steps RKF steps of z_range/num_steps, all
+ * accepted (I += delta4 of integration.cl:63-79, k1 carried from the previous
+ * step). No reference counterpart as an entry point: it is the reference's
+ * integrator with the step controller removed. */
+ilc_status ilc_render_fixed(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                            int64_t num_steps, const ilc_los_scaling* scaling, float* image,
+                            int is_device, ilc_render_stats* stats);
+
+/* The multiplier applied to every pixel by volumetric_integration.cpp:74-87. */
+float ilc_los_scale(const ilc_camera* cam, double z_range, const ilc_los_scaling* scaling);
+
+/* The band-map pipeline of `illcrawl_render -t image -q xray_flux` in one call:
+ * reconstructing_data_crawler::run's first pass (reconstructing_data_crawler.cpp:157-256:
+ * per-cell xray_flux by quantity_transformation, packed into the particles'
+ * q, then setup_particles) followed by create_projection. cells: n float4
+ * records (x, y, z, unused); rho, u, xe: n floats. The grid built here stays
+ * on the context, as the crawler keeps it for later runs. */
+ilc_status ilc_project_xray_flux(ilc_ctx* ctx, const float* cells, const float* rho,
+                                 const float* u, const float* xe, uint64_t n, float redshift,
+                                 float luminosity_distance, float e_min, float e_max,
+                                 int32_t num_samples, const ilc_camera* cam, double z_range,
+                                 ilc_tolerance tol, int32_t controller,
+                                 const ilc_los_scaling* scaling, float* image, int is_device,
+                                 ilc_render_stats* stats);
+
+/* Number of kernels this context has launched so far. */
+uint64_t ilc_kernel_launches(const ilc_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ILC_H */

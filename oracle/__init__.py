@@ -1,0 +1,214 @@
+"""ctypes bindings to the CPU oracle (``oracle/libilc_oracle.so``).
+
+Test infrastructure only: imported by ``tests/``, by ``__graft_entry__.smoke()``
+and by the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py``, where
+it is the checker and the timed CPU restatement. The product package
+``illcrawl_b200`` never imports this module.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libilc_oracle.so")
+_lib = None
+
+
+class OracleCamera(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_double * 3), ("look_at", ctypes.c_double * 3),
+                ("roll", ctypes.c_double), ("screen_width", ctypes.c_double),
+                ("nx", ctypes.c_int32), ("ny", ctypes.c_int32)]
+
+
+def build():
+    """Compile the oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    P = ctypes.c_void_p
+    i64, i32, f32, f64 = ctypes.c_int64, ctypes.c_int32, ctypes.c_float, ctypes.c_double
+    L.orc_spiral_table.argtypes = [P]
+    L.orc_logf.argtypes = [f32]; L.orc_logf.restype = f32
+    L.orc_expf.argtypes = [f32]; L.orc_expf.restype = f32
+    L.orc_grid_build.argtypes = [P, i64, P]; L.orc_grid_build.restype = P
+    L.orc_grid_free.argtypes = [P]
+    L.orc_grid_info.argtypes = [P, P, P, P, P]
+    L.orc_grid_export.argtypes = [P, P, P, P, P]
+    L.orc_nn8_query.argtypes = [P, P, i64, ctypes.c_int, P, P, P, P, ctypes.c_int]
+    L.orc_camera_setup.argtypes = [P, P]
+    L.orc_render.argtypes = [P, P, f64, f64, f64, ctypes.c_int, i64, P, i64, P, P, P, P,
+                             ctypes.c_int]
+    L.orc_render_fixed.argtypes = [P, P, f64, i64, ctypes.c_int, P, i64, P, P, ctypes.c_int]
+    L.orc_render_record.argtypes = [P, P, f64, f64, f64, ctypes.c_int, i64, P, i64, P, P, i64,
+                                    P, ctypes.c_int]
+    L.orc_render_replay.argtypes = [P, P, P, i64, P, i64, P, ctypes.c_int, P, ctypes.c_int]
+    L.orc_los_scale.argtypes = [P, f64, f64, f64, ctypes.c_int]; L.orc_los_scale.restype = f32
+    L.orc_gaunt_lookup.argtypes = [P, ctypes.c_int, ctypes.c_int, f32, f32]
+    L.orc_gaunt_lookup.restype = f32
+    L.orc_temperature.argtypes = [P, P, i64, P]
+    L.orc_xray_band.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, i64, f32, f32, f32, f32,
+                                ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
+    L.orc_xray_bin.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, i64, f32, f32, f32, f32,
+                               ctypes.c_int, P, ctypes.c_int]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def camera(position, look_at, roll, screen_width, nx, ny):
+    c = OracleCamera()
+    c.position[:] = [float(v) for v in position]
+    c.look_at[:] = [float(v) for v in look_at]
+    c.roll, c.screen_width, c.nx, c.ny = float(roll), float(screen_width), int(nx), int(ny)
+    return c
+
+
+def spiral_table():
+    out = np.zeros((8, 125, 3), np.int8)
+    lib().orc_spiral_table(_p(out))
+    return out
+
+
+def logf(x):
+    return np.float32(lib().orc_logf(float(x)))
+
+
+def expf(x):
+    return np.float32(lib().orc_expf(float(x)))
+
+
+class Grid:
+    """Grid built by the oracle from float4 (x, y, z, q) particles."""
+
+    def __init__(self, xyzq):
+        self.xyzq = np.ascontiguousarray(xyzq, np.float32).reshape(-1, 4)
+        st = ctypes.c_int32(0)
+        self.h = lib().orc_grid_build(_p(self.xyzq), self.xyzq.shape[0], ctypes.byref(st))
+        if not self.h:
+            raise ValueError(f"oracle grid build failed (status {st.value})")
+        mn = np.zeros(3, np.float32); cs = np.zeros(3, np.float32)
+        n3 = np.zeros(3, np.int32); tot = np.zeros(1, np.uint64)
+        lib().orc_grid_info(self.h, _p(mn), _p(cs), _p(n3), _p(tot))
+        self.min_corner, self.cell_sizes, self.num_cells = mn, cs, n3
+        self.total_cells = int(tot[0])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_grid_free(self.h)
+            self.h = None
+
+    def export(self):
+        n = self.xyzq.shape[0]
+        cells = np.zeros((self.total_cells, 2), np.int32)
+        s2u = np.zeros(n, np.uint32)
+        srt = np.zeros((n, 4), np.float32)
+        keys = np.zeros(n, np.uint64)
+        lib().orc_grid_export(self.h, _p(cells), _p(s2u), _p(srt), _p(keys))
+        return cells, s2u, srt, keys
+
+    def nn8(self, pts, precision=0, nthreads=0, slots=True):
+        pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 4)
+        n = pts.shape[0]
+        out = np.zeros(n, np.float32)
+        idx = np.zeros((n, 8), np.int32) if slots else None
+        d8 = np.zeros((n, 8), np.float32) if slots else None
+        st = np.zeros(2, np.uint64)
+        lib().orc_nn8_query(self.h, _p(pts), n, precision, _p(out), _p(idx), _p(d8), _p(st),
+                            nthreads)
+        return out, idx, d8, st
+
+    def render(self, cam, z_range, atol, rtol, mode=0, pix=None, max_steps=1 << 22, nthreads=0):
+        npix = cam.nx * cam.ny if pix is None else len(pix)
+        pixa = None if pix is None else np.ascontiguousarray(pix, np.int64)
+        out = np.zeros(npix, np.float32)
+        steps = np.zeros(npix, np.int32); acc = np.zeros(npix, np.int32)
+        st = np.zeros(2, np.uint64)
+        rc = lib().orc_render(self.h, ctypes.byref(cam), z_range, atol, rtol, mode, max_steps,
+                              _p(pixa), npix, _p(out), _p(steps), _p(acc), _p(st), nthreads)
+        return out, steps, acc, st, rc
+
+    def render_fixed(self, cam, z_range, n_steps, precision=0, pix=None, nthreads=0):
+        npix = cam.nx * cam.ny if pix is None else len(pix)
+        pixa = None if pix is None else np.ascontiguousarray(pix, np.int64)
+        out = np.zeros(npix, np.float32)
+        st = np.zeros(2, np.uint64)
+        lib().orc_render_fixed(self.h, ctypes.byref(cam), z_range, n_steps, precision,
+                               _p(pixa), npix, _p(out), _p(st), nthreads)
+        return out, st
+
+    def render_record(self, cam, z_range, atol, rtol, mode=0, pix=None, cap=4096,
+                      max_steps=1 << 22, nthreads=0):
+        npix = cam.nx * cam.ny if pix is None else len(pix)
+        pixa = None if pix is None else np.ascontiguousarray(pix, np.int64)
+        out = np.zeros(npix, np.float32)
+        hs = np.zeros((npix, cap), np.float32)
+        n = np.zeros(npix, np.int32)
+        rc = lib().orc_render_record(self.h, ctypes.byref(cam), z_range, atol, rtol, mode,
+                                     max_steps, _p(pixa), npix, _p(out), _p(hs), cap, _p(n),
+                                     nthreads)
+        return out, hs, n, rc
+
+    def render_replay(self, cam, hs, n, pix=None, precision=0, nthreads=0):
+        hs = np.ascontiguousarray(hs, np.float32)
+        npix = hs.shape[0]
+        pixa = None if pix is None else np.ascontiguousarray(pix, np.int64)
+        n = np.ascontiguousarray(n, np.int32)
+        out = np.zeros(npix, np.float32)
+        lib().orc_render_replay(self.h, ctypes.byref(cam), _p(pixa), npix, _p(hs), hs.shape[1],
+                                _p(n), precision, _p(out), nthreads)
+        return out
+
+
+def camera_setup(cam):
+    out = np.zeros(13, np.float32)
+    lib().orc_camera_setup(ctypes.byref(cam), _p(out))
+    return out
+
+
+def los_scale(cam, z_range, length_conv=1.0, area_conv=1.0, dA_mode=0):
+    return np.float32(lib().orc_los_scale(ctypes.byref(cam), z_range, length_conv, area_conv,
+                                          dA_mode))
+
+
+def gaunt_lookup(table, lg, lu):
+    t = np.ascontiguousarray(table, np.float32)
+    return np.float32(lib().orc_gaunt_lookup(_p(t), t.shape[1], t.shape[0], float(lg), float(lu)))
+
+
+def temperature(u, xe):
+    u = np.ascontiguousarray(u, np.float32); xe = np.ascontiguousarray(xe, np.float32)
+    out = np.zeros_like(u)
+    lib().orc_temperature(_p(u), _p(xe), u.size, _p(out))
+    return out
+
+
+def xray_band(table, rho, u, xe, z, dL, Emin, Emax, num_samples, precision=0, nthreads=0):
+    t = np.ascontiguousarray(table, np.float32)
+    rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+    out = np.zeros_like(rho)
+    lib().orc_xray_band(_p(t), t.shape[1], t.shape[0], _p(rho), _p(u), _p(xe), rho.size, z, dL,
+                        Emin, Emax, num_samples, precision, _p(out), nthreads)
+    return out
+
+
+def xray_bin(table, rho, u, xe, z, dL, E, dE, precision=0, nthreads=0):
+    t = np.ascontiguousarray(table, np.float32)
+    rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+    out = np.zeros_like(rho)
+    lib().orc_xray_bin(_p(t), t.shape[1], t.shape[0], _p(rho), _p(u), _p(xe), rho.size, z, dL,
+                       E, dE, precision, _p(out), nthreads)
+    return out
