@@ -153,7 +153,7 @@ def run_reference(args, rank, world):
             "ms_per_step": NX * NY / (v * 1e6) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded NFW + uniform gas cells)",
-            "config": {"workload": WORKLOAD, "cells": 4194304, "image": [NX, NY],
+            "config": {"workload": f"xray_band_map_4M_cells_{NX}sq_rtol1e-3", "cells": 4194304, "image": [NX, NY],
                        "rel_tol": REL_TOL},
             "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "port",
                              "sample": f"per step: per-cell X-ray flux + grid build over all "
@@ -232,22 +232,26 @@ def run_ours(args, rank, world, local_rank):
                                      num_samples=NUM_SAMPLES, scaling=scaling,
                                      image=h_img.numpy())
 
-    e2e_step()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e2e_steps = max(1, min(args.steps, 2))
-    for _ in range(e2e_steps):
-        flush.fill_(2.0)
-        torch.cuda.synchronize()
+    e2e_value = None
+    if not args.no_e2e:
         e2e_step()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = rays / e2e_s / 1e6
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e2e_steps = max(1, min(args.steps, 2))
+        e2e_s = 0.0
+        for _ in range(e2e_steps):
+            flush.fill_(2.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e2e_step()
+            e2e_s += time.perf_counter() - t0
+        e2e_s /= e2e_steps
+        if dist:
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_value = rays / e2e_s / 1e6
 
     if rank != 0:
         ctx.close()
@@ -256,13 +260,13 @@ def run_ours(args, rank, world, local_rank):
     kbytes = algorithmic_bytes(last_stats, n, NX * NY)
     achieved = kbytes / (last_stats["kernel_ms"] * 1e-3) / 1e9
     cores = os.cpu_count() or 1
-    cpu_v, tf, tr = cpu_baseline(cells, cores)
+    cpu_v = None if args.no_cpu else cpu_baseline(cells, cores)[0]
     line = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded NFW + uniform gas cells, numpy PCG64 seed 20171)",
-        "config": {"workload": WORKLOAD, "cells": n, "image": [NX, NY], "z_range_kpc": BOX,
+        "config": {"workload": f"xray_band_map_4M_cells_{NX}sq_rtol1e-3", "cells": n, "image": [NX, NY], "z_range_kpc": BOX,
                    "rel_tol": REL_TOL, "controller": "fp64", "band_keV": [E_MIN, E_MAX],
                    "parallelism": f"replicas x{world}",
                    "l2": "flushed by a 256 MiB write before every step"},
@@ -289,7 +293,13 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--image", type=int, default=1024,
+                    help="image side in pixels (1024 = the benchmark; smaller only for profiling)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
     args = ap.parse_args()
+    global NX, NY
+    NX = NY = args.image
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

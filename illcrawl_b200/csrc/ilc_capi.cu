@@ -310,7 +310,8 @@ ilc_status ilc_nn8_setup_particles(ilc_ctx* h, const float* particles, uint64_t 
   if (flags & FLAG_KEY_RANGE) return fail(c, ILC_ERR_INTERNAL, "particle outside its grid");
   c.n_particles = n;
   c.has_grid = true;
-  c.list_n = 0;
+  // The nn8 lists survive a new particle block: the next query with
+  // merge_previous = 1 continues them (reconstructing_data_crawler.cpp:164-255).
   return ILC_OK;
 }
 

@@ -9,6 +9,7 @@
 // compaction, without its per-iteration host synchronisations.
 #include "ilc_device.cuh"
 #include "ilc_internal.h"
+#include "ilc_walk4.cuh"
 
 namespace ilc {
 
@@ -40,15 +41,17 @@ struct RenderK {
   float* out;
 };
 
-// Pixel tiling: a block covers 16 x 16 pixels; each warp an 8 x 4 tile, so
-// the 32 rays of a warp are spatial neighbours.
+// Pixel tiling: a block of 128 threads covers 16 x 8 pixels; each warp an
+// 8 x 4 tile, so the 32 rays of a warp are spatial neighbours.
+constexpr int kRenderThreads = 128;
+constexpr int kTileX = 16, kTileY = 8;
 __device__ __forceinline__ void block_pixel(int& ix, int& iy) {
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  ix = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-  iy = blockIdx.y * 16 + (warp >> 1) * 4 + (lane >> 3);
+  ix = blockIdx.x * kTileX + (warp & 1) * 8 + (lane & 7);
+  iy = blockIdx.y * kTileY + (warp >> 1) * 4 + (lane >> 3);
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kRenderThreads)
 render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
               uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
   __shared__ char4 spiral[1000];
@@ -71,9 +74,7 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
       for (int64_t s = 0; s < a.fixed_steps; ++s) {
         rkf_points(z, h, pts);
         float e[4];
-#pragma unroll 1
-        for (int j = 0; j < 4; ++j)
-          e[j] = nn8_value(g, spiral, px + pts[j] * lx, py + pts[j] * ly, pz + pts[j] * lz, ws);
+        nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
         float d4 = 25.f / 216.f * k1 + 1408.f / 2565.f * e[0] + 2197.f / 4101.f * e[1] -
                    1.f / 5.f * e[2];
         d4 *= h;
@@ -88,9 +89,7 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
       while (z < a.z_end) {
         if ((int64_t)steps >= a.max_steps) { at_limit = true; break; }
         float e[4];
-#pragma unroll 1
-        for (int j = 0; j < 4; ++j)
-          e[j] = nn8_value(g, spiral, px + pts[j] * lx, py + pts[j] * ly, pz + pts[j] * lz, ws);
+        nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
         const float zb = z;
         if (a.controller == ILC_CONTROLLER_REF32)
           rkf_advance_ref32(I, z, h, k1, fa, fr, a.z_end, e, kEps, kHmin, kHmax, pts);
@@ -149,13 +148,13 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   k.apply_scale = a.apply_scale ? 1 : 0;
   k.out = a.out;
   const GridView g = make_grid_view(c);
-  dim3 grid((a.nx + 15) / 16, (a.ny + 15) / 16);
+  dim3 grid((a.nx + kTileX - 1) / kTileX, (a.ny + kTileY - 1) / kTileY);
   if (!c.ev0) {
     if ((e = cudaEventCreate(&c.ev0)) || (e = cudaEventCreate(&c.ev1))) return e;
   }
   cudaEventRecord(c.ev0, c.stream);
   ++c.launches;
-  render_kernel<<<grid, 256, 0, c.stream>>>(
+  render_kernel<<<grid, kRenderThreads, 0, c.stream>>>(
       k, g, c.spiral.as<char4>(), c.flags.as<uint32_t>(),
       reinterpret_cast<unsigned long long*>(c.flags.as<char>() + 64));
   if ((e = cudaGetLastError())) return e;

@@ -1,0 +1,219 @@
+// ilc_walk4.cuh -- the nn8 walk for the 4 integrand points of one RKF step,
+// done as one pass over the grid.
+//
+// The 4 points of a step lie within one step length (typically < 1 kpc) of
+// each other, so almost always in the same grid cell and subcell: they then
+// share the reference's spiral cell order, and one walk serves all four. Each
+// point keeps its own 8 slots, its own search radius and its own early break
+// (volumetric_nn8_reconstruction.cl:157-171): a point stops taking part at the
+// cell where its own break condition holds, exactly as its single-point walk
+// would. Every point therefore sees the same cells and candidates in the same
+// order as alone, and its slots evolve identically -- the result is the
+// reference's, bit for bit. What is shared is the spiral/cell bookkeeping and
+// the candidate loads (one 16-byte load serves four distance tests). Points in
+// a different cell or subcell are walked in a further pass.
+//
+// Distances for pairs of points are evaluated with sm_100's paired fp32
+// instructions (__fadd2_rn / __fmul2_rn): each lane of the pair is an IEEE
+// round-to-nearest add or multiply, so the results equal the scalar
+// (x*x + y*y) + z*z of the reference's op order.
+#pragma once
+
+#include "ilc_device.cuh"
+
+namespace ilc {
+
+struct Step4 {
+  float qx[4], qy[4], qz[4];
+  float d[4][8], v[4][8];
+  float R[4], R2up[4];
+  int mi[4], cnt[4];
+};
+
+template <int J> __device__ __forceinline__ void s4_rescan(Step4& s) {
+  float r = 0.0f;
+  int m = 0;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    if (s.d[J][t] > r) m = t;
+    r = fmaxf(r, s.d[J][t]);
+  }
+  s.R[J] = r;
+  s.mi[J] = m;
+  s.R2up[J] = __fmul_ru(r, r);
+}
+
+template <int J> __device__ __forceinline__ void s4_init(Step4& s) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t) { s.d[J][t] = FLT_MAX; s.v[J][t] = 0.0f; }
+  s.R[J] = FLT_MAX;
+  s.R2up[J] = __int_as_float(0x7f800000);
+  s.mi[J] = 0;
+  s.cnt[J] = 0;
+}
+
+// Insertion into point J's slots. While fewer than 8 slots are filled the
+// search radius is FLT_MAX and the first-max slot is the next empty one, so
+// the k-th accepted candidate goes to slot k without a rescan; the 8th
+// insertion rescans. Afterwards: replace the first-max slot and rescan.
+template <int J> __device__ __forceinline__ void s4_insert(Step4& s, float dist, float val) {
+  if (s.cnt[J] < 8) {
+    const int k = s.cnt[J];
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t == k) { s.d[J][t] = dist; s.v[J][t] = val; }
+    s.cnt[J] = k + 1;
+    if (k == 7) s4_rescan<J>(s);
+  } else {
+    const int m = s.mi[J];
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t == m) { s.d[J][t] = dist; s.v[J][t] = val; }
+    s4_rescan<J>(s);
+  }
+}
+
+template <int J>
+__device__ __forceinline__ void s4_test(Step4& s, unsigned act, float d2, float val) {
+  if ((act >> J) & 1u) {
+    if (d2 <= s.R2up[J]) {
+      const float dist = sqrtf(d2);
+      if (dist < s.R[J]) s4_insert<J>(s, dist, val);
+    }
+  }
+}
+
+template <int J> __device__ __forceinline__ float s4_finalize(const Step4& s) {
+  float w[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) w[t] = weight3d(s.d[J][t]);
+  float ws = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) ws = ws + w[t];
+  float dot = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) dot = __fmaf_rn(w[t], s.v[J][t], dot);
+  float res = 0.0f;
+  if (ws != 0.0f && dot != 0.0f) res = dot / ws;
+  return res;
+}
+
+// One walk over the spiral of (cx, cy, cz, sub) for the points in `mask`.
+__device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict__ spiral,
+                                      Step4& s, unsigned mask, int cx, int cy, int cz, int sub,
+                                      WalkStats& st) {
+  const char4* order = spiral + sub * 125;
+  const float2 nqx01 = make_float2(-s.qx[0], -s.qx[1]), nqx23 = make_float2(-s.qx[2], -s.qx[3]);
+  const float2 nqy01 = make_float2(-s.qy[0], -s.qy[1]), nqy23 = make_float2(-s.qy[2], -s.qy[3]);
+  const float2 nqz01 = make_float2(-s.qz[0], -s.qz[1]), nqz23 = make_float2(-s.qz[2], -s.qz[3]);
+  const float2 crad = make_float2(g.cell_radius, g.cell_radius);
+  unsigned act = mask;
+  for (int it = 0; it < 125; ++it) {
+    const char4 o = order[it];
+    const int ix = cx + o.x, iy = cy + o.y, iz = cz + o.z;
+    const float ccx = (g.min0 + (float)ix * g.cs0) + g.half0;
+    const float ccy = (g.min1 + (float)iy * g.cs1) + g.half1;
+    const float ccz = (g.min2 + (float)iz * g.cs2) + g.half2;
+    {
+      // early break per point: |c - q|^2 > (R + cell_radius)^2
+      const float2 cx2 = make_float2(ccx, ccx), cy2 = make_float2(ccy, ccy),
+                   cz2 = make_float2(ccz, ccz);
+      float2 ex = __fadd2_rn(cx2, nqx01), ey = __fadd2_rn(cy2, nqy01), ez = __fadd2_rn(cz2, nqz01);
+      const float2 dd01 = __fadd2_rn(__fadd2_rn(__fmul2_rn(ex, ex), __fmul2_rn(ey, ey)),
+                                     __fmul2_rn(ez, ez));
+      ex = __fadd2_rn(cx2, nqx23); ey = __fadd2_rn(cy2, nqy23); ez = __fadd2_rn(cz2, nqz23);
+      const float2 dd23 = __fadd2_rn(__fadd2_rn(__fmul2_rn(ex, ex), __fmul2_rn(ey, ey)),
+                                     __fmul2_rn(ez, ez));
+      const float2 r01 = __fadd2_rn(make_float2(s.R[0], s.R[1]), crad);
+      const float2 r23 = __fadd2_rn(make_float2(s.R[2], s.R[3]), crad);
+      const float2 rr01 = __fmul2_rn(r01, r01), rr23 = __fmul2_rn(r23, r23);
+      unsigned brk = (dd01.x > rr01.x ? 1u : 0u) | (dd01.y > rr01.y ? 2u : 0u) |
+                     (dd23.x > rr23.x ? 4u : 0u) | (dd23.y > rr23.y ? 8u : 0u);
+      act &= ~brk;
+    }
+    if (!act) break;
+    if ((unsigned)ix >= (unsigned)g.n0 || (unsigned)iy >= (unsigned)g.n1 ||
+        (unsigned)iz >= (unsigned)g.n2)
+      continue;
+    const size_t key = (size_t)ix + (size_t)iy * (size_t)g.n0 +
+                       (size_t)iz * (size_t)g.n0 * (size_t)g.n1;
+    const int2 be = __ldg(&g.cells[key]);
+    const unsigned na = __popc(act);
+    st.cells += na;
+    st.cands += na * (uint32_t)max(be.y - be.x, 0);
+    for (int p = be.x; p < be.y; ++p) {
+      const float4 P = __ldg(&g.parts[p]);
+      const float2 px = make_float2(P.x, P.x), py = make_float2(P.y, P.y),
+                   pz = make_float2(P.z, P.z);
+      float2 fx = __fadd2_rn(px, nqx01), fy = __fadd2_rn(py, nqy01), fz = __fadd2_rn(pz, nqz01);
+      const float2 d01 = __fadd2_rn(__fadd2_rn(__fmul2_rn(fx, fx), __fmul2_rn(fy, fy)),
+                                    __fmul2_rn(fz, fz));
+      fx = __fadd2_rn(px, nqx23); fy = __fadd2_rn(py, nqy23); fz = __fadd2_rn(pz, nqz23);
+      const float2 d23 = __fadd2_rn(__fadd2_rn(__fmul2_rn(fx, fx), __fmul2_rn(fy, fy)),
+                                    __fmul2_rn(fz, fz));
+      s4_test<0>(s, act, d01.x, P.w);
+      s4_test<1>(s, act, d01.y, P.w);
+      s4_test<2>(s, act, d23.x, P.w);
+      s4_test<3>(s, act, d23.y, P.w);
+    }
+  }
+}
+
+// Cell and subcell of a point (volumetric_nn8_reconstruction.cl:129-155).
+__device__ __forceinline__ void locate(const GridView& g, float qx, float qy, float qz, int& cx,
+                                       int& cy, int& cz, int& sub) {
+  cx = clamp_cell(to_int_sat(floorf((qx - g.min0) / g.cs0)));
+  cy = clamp_cell(to_int_sat(floorf((qy - g.min1) / g.cs1)));
+  cz = clamp_cell(to_int_sat(floorf((qz - g.min2) / g.cs2)));
+  const float mx = g.min0 + (float)cx * g.cs0;
+  const float my = g.min1 + (float)cy * g.cs1;
+  const float mz = g.min2 + (float)cz * g.cs2;
+  int sx = to_int_sat(floorf((qx - mx) / g.half0));
+  int sy = to_int_sat(floorf((qy - my) / g.half1));
+  int sz = to_int_sat(floorf((qz - mz) / g.half2));
+  sx = min(max(sx, 0), 1);
+  sy = min(max(sy, 0), 1);
+  sz = min(max(sz, 0), 1);
+  sub = sx + 2 * sy + 4 * sz;
+}
+
+// nn8 values of the 4 points of one step (e[j] for point j).
+__device__ __forceinline__ void nn8_step4(const GridView& g, const char4* __restrict__ spiral,
+                                          float px, float py, float pz, float lx, float ly,
+                                          float lz, const float zq[4], float e[4],
+                                          WalkStats& st) {
+  Step4 s;
+  int cx[4], cy[4], cz[4], sb[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    s.qx[j] = px + zq[j] * lx;
+    s.qy[j] = py + zq[j] * ly;
+    s.qz[j] = pz + zq[j] * lz;
+    locate(g, s.qx[j], s.qy[j], s.qz[j], cx[j], cy[j], cz[j], sb[j]);
+  }
+  s4_init<0>(s);
+  s4_init<1>(s);
+  s4_init<2>(s);
+  s4_init<3>(s);
+  unsigned todo = 0xFu;
+  while (todo) {
+    const int j0 = __ffs(todo) - 1;
+    int c0x = cx[0], c0y = cy[0], c0z = cz[0], s0 = sb[0];
+#pragma unroll
+    for (int j = 1; j < 4; ++j)
+      if (j == j0) { c0x = cx[j]; c0y = cy[j]; c0z = cz[j]; s0 = sb[j]; }
+    unsigned mask = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (((todo >> j) & 1u) && cx[j] == c0x && cy[j] == c0y && cz[j] == c0z && sb[j] == s0)
+        mask |= 1u << j;
+    walk4(g, spiral, s, mask, c0x, c0y, c0z, s0, st);
+    todo &= ~mask;
+  }
+  e[0] = s4_finalize<0>(s);
+  e[1] = s4_finalize<1>(s);
+  e[2] = s4_finalize<2>(s);
+  e[3] = s4_finalize<3>(s);
+}
+
+}  // namespace ilc

@@ -1,0 +1,124 @@
+// ilc_backend.hpp -- C++ adapter of the B200 backend to illcrawl's interfaces.
+//
+// Header-only, over the C ABI of ilc.h. It mirrors:
+//   * reconstruction_backend / reconstruction_backends::nn8
+//     (reconstruction_backend.hpp:35-58, volumetric_reconstruction_backend_nn8.hpp:36-82):
+//     class nn8_cuda, with a device_view (pointer + count) in place of cl::Buffer;
+//   * volumetric_integration::create_projection (volumetric_integration.cpp:32-88):
+//     function create_projection, which runs the whole RKF loop on the device.
+// Errors are reported as exceptions (ilc::error), as the reference's
+// qcl::check_cl_error / std::runtime_error do.
+#ifndef ILC_BACKEND_HPP
+#define ILC_BACKEND_HPP
+
+#include <array>
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "ilc.h"
+
+namespace ilc {
+
+class error : public std::runtime_error {
+ public:
+  error(ilc_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+  ilc_status status;
+};
+
+// Owning handle of an ilc_ctx (one device, one stream).
+class context {
+ public:
+  explicit context(int device = 0) : h_(ilc_create(device)) {
+    if (!h_) throw error(ILC_ERR_CUDA, "ilc_create failed: no usable CUDA device");
+  }
+  ~context() { ilc_destroy(h_); }
+  context(const context&) = delete;
+  context& operator=(const context&) = delete;
+  ilc_ctx* get() const { return h_; }
+  void check(ilc_status s) const {
+    if (s != ILC_OK) throw error(s, ilc_last_error(h_));
+  }
+
+ private:
+  ilc_ctx* h_;
+};
+
+// A caller-owned array; on_device selects the pointer kind (ilc.h "is_device").
+template <class T> struct view {
+  T* ptr = nullptr;
+  std::size_t n = 0;
+  bool on_device = false;
+};
+
+// float4 particle record, the reference's device_vector4 (x, y, z, quantity).
+struct particle {
+  float s[4];
+};
+
+// reconstruction_backends::nn8 over the CUDA context.
+class nn8_cuda {
+ public:
+  explicit nn8_cuda(context& ctx) : ctx_(ctx) {}
+  virtual ~nn8_cuda() {}
+
+  // No smoothing lengths or other per-particle datasets are needed
+  // (volumetric_reconstruction_backend_nn8.cpp:32-35).
+  std::vector<std::string> get_required_additional_datasets() const { return {}; }
+  std::string get_backend_name() const { return "volumetric/nn8_cuda"; }
+  void init_backend(std::size_t blocksize) { blocksize_ = blocksize; }
+
+  void setup_particles(const std::vector<particle>& particles) {
+    ctx_.check(ilc_nn8_setup_particles(ctx_.get(), &particles[0].s[0], particles.size(), 0));
+  }
+  void setup_particles(view<const float> particles_float4) {
+    ctx_.check(ilc_nn8_setup_particles(ctx_.get(), particles_float4.ptr, particles_float4.n,
+                                       particles_float4.on_device ? 1 : 0));
+  }
+
+  // Borrowed until the next setup_evaluation_points, as the reference's cl::Buffer.
+  void setup_evaluation_points(view<const float> points_float4, std::size_t num_points) {
+    points_ = points_float4;
+    n_ = num_points;
+    first_run_ = true;
+    result_.assign(num_points, 0.0f);
+  }
+
+  // One particle block; later blocks merge into the running lists.
+  void run() {
+    ctx_.check(ilc_nn8_query(ctx_.get(), points_.ptr, n_, first_run_ ? 0 : 1, result_.data(),
+                             nullptr, nullptr, points_.on_device ? 1 : 0));
+    first_run_ = false;
+  }
+
+  const std::vector<float>& retrieve_results() const { return result_; }
+
+ private:
+  context& ctx_;
+  std::size_t blocksize_ = 0;
+  view<const float> points_;
+  std::size_t n_ = 0;
+  bool first_run_ = true;
+  std::vector<float> result_;
+};
+
+// volumetric_integration::create_projection: output is num_pix_x * num_pix_y
+// floats, row = y; quantities pick dA_mode as their
+// effective_line_of_sight_integration_dA does.
+inline ilc_render_stats create_projection(context& ctx, const ilc_camera& cam, double z_range,
+                                          double abs_tol, double rel_tol,
+                                          const ilc_los_scaling& scaling, std::vector<float>& out,
+                                          int controller = ILC_CONTROLLER_FP64) {
+  out.assign((std::size_t)cam.num_pix_x * (std::size_t)cam.num_pix_y, 0.0f);
+  ilc_render_stats st{};
+  ctx.check(ilc_render_adaptive(ctx.get(), &cam, z_range, ilc_tolerance{abs_tol, rel_tol},
+                                controller, &scaling, out.data(), 0, &st));
+  return st;
+}
+
+}  // namespace ilc
+
+#endif  // ILC_BACKEND_HPP

@@ -212,3 +212,28 @@ def xray_bin(table, rho, u, xe, z, dL, E, dE, precision=0, nthreads=0):
     lib().orc_xray_bin(_p(t), t.shape[1], t.shape[0], _p(rho), _p(u), _p(xe), rho.size, z, dL,
                        E, dE, precision, _p(out), nthreads)
     return out
+
+
+def _declare_lists(L):
+    P = ctypes.c_void_p
+    L.orc_nn8_query_lists.argtypes = [P, P, ctypes.c_int64, ctypes.c_int, P, P, P, P,
+                                      ctypes.c_int]
+
+
+def nn8_lists(grid, pts, merge=False, lists=None, nthreads=0):
+    """nn8 with explicit running lists (d, v, original id), as the reference's
+    multi-block merge. Returns (values, (list_d, list_v, list_id))."""
+    L = lib()
+    if not getattr(L, "_lists_declared", False):
+        _declare_lists(L)
+        L._lists_declared = True
+    pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 4)
+    n = pts.shape[0]
+    if lists is None:
+        lists = (np.zeros((n, 8), np.float32), np.zeros((n, 8), np.float32),
+                 np.zeros((n, 8), np.int32))
+    ld, lv, li = (np.ascontiguousarray(a) for a in lists)
+    out = np.zeros(n, np.float32)
+    L.orc_nn8_query_lists(grid.h, _p(pts), n, int(merge), _p(ld), _p(lv), _p(li), _p(out),
+                          nthreads)
+    return out, (ld, lv, li)

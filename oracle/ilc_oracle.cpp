@@ -834,6 +834,40 @@ int orc_nn8_query(void* h, const float* pts, int64_t n, int precision, float* ou
   return 0;
 }
 
+// nn8 with explicit running lists (fp32): merge = 0 starts from empty lists,
+// merge = 1 continues list_d / list_v / list_id (n x 8, original indices), as
+// the reference's multi-block reconstruction (volumetric_nn8_reconstruction.cl:112-126).
+int orc_nn8_query_lists(void* h, const float* pts, int64_t n, int merge, float* list_d,
+                        float* list_v, int32_t* list_id, float* out, int nthreads) {
+  Grid* g = (Grid*)h;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < n; ++i) {
+    const float* q = pts + 4 * i;
+    Slots<float> s;
+    if (merge) {
+      for (int j = 0; j < 8; ++j) {
+        s.d[j] = list_d[8 * i + j];
+        s.v[j] = list_v[8 * i + j];
+        const int32_t o = list_id[8 * i + j];
+        s.id[j] = o >= 0 ? (int32_t)(0x80000000u | (uint32_t)o) : -1;
+      }
+    } else {
+      slots_init(s);
+    }
+    nn8_search<float>(*g, q[0], q[1], q[2], s, nullptr);
+    out[i] = nn8_finalize(s);
+    for (int j = 0; j < 8; ++j) {
+      const int32_t id = s.id[j];
+      list_d[8 * i + j] = s.d[j];
+      list_v[8 * i + j] = s.v[j];
+      list_id[8 * i + j] =
+          id == -1 ? -1 : (id < 0 ? (int32_t)((uint32_t)id & 0x7fffffffu) : (int32_t)g->s2u[id]);
+    }
+  }
+  return 0;
+}
+
 // Camera basis as the device receives it: look, b0, b1, min corner (float) + pixel size.
 int orc_camera_setup(const orc_camera* c, float* out13) {
   Camera cam;
