@@ -29,6 +29,8 @@ sys.path.insert(0, ROOT)
 METRIC = "Mrays/s (X-ray map, 1e-3 tol)"
 NX = NY = 1024
 BOX = 6000.0
+Z_START = 0.0      # camera plane along z (0: the face of the cube)
+DEPTH = BOX        # integration depth
 REL_TOL = 1e-3
 E_MIN, E_MAX, NUM_SAMPLES = 0.5, 7.0, 100
 REDSHIFT, DL = 0.2, 978500.0
@@ -93,6 +95,32 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+TUNING_FILE = os.path.join(ROOT, "illcrawl_b200", "data", "render_tuning.json")
+
+
+def tune_schedule(ctx, cam, args, gpu_name):
+    """z window of the adaptive render: --z-window if given, else the cached
+    autotuner result for this workload and GPU, else run the autotuner (a
+    sample of tile rows per candidate, outside the timed region) and cache."""
+    import illcrawl_b200 as ilc
+    if args.z_window is not None:
+        ctx.set_z_window(args.z_window)
+        return {"z_window": args.z_window, "source": "command line"}
+    key = f"{gpu_name}|xray_band_map_4M_cells_{NX}sq_rtol1e-3|z0={Z_START}|depth={DEPTH}"
+    cache = json.load(open(TUNING_FILE)) if os.path.exists(TUNING_FILE) else {}
+    if key in cache:
+        ctx.set_z_window(cache[key]["z_window"])
+        return dict(cache[key], source="cache")
+    best, times = ctx.autotune_z_window(cam, DEPTH, REL_TOL, 0.0, ilc.CONTROLLER_FP64,
+                                        sample_stride=max(1, NY // 64))
+    cache[key] = {"z_window": best, "kernel_ms": times}
+    try:
+        json.dump(cache, open(TUNING_FILE, "w"), indent=1, sort_keys=True)
+    except OSError:
+        pass
+    return dict(cache[key], source="autotuner")
+
+
 def make_inputs():
     from illcrawl_b200 import synthetic
     cells = synthetic.xray_cells()
@@ -101,7 +129,7 @@ def make_inputs():
 
 
 def camera_args():
-    return ((BOX / 2, BOX / 2, 0.0), (0.0, 0.0, 1.0), 0.0, BOX, NX, NY)
+    return ((BOX / 2, BOX / 2, Z_START), (0.0, 0.0, 1.0), 0.0, BOX * NX / 1024, NX, NY)
 
 
 def algorithmic_bytes(st, n_cells, n_rays):
@@ -124,7 +152,7 @@ def cpu_baseline(cells, nthreads, sample_rays=2048, seed=1):
     t_fixed = time.perf_counter() - t0
     pix = np.random.default_rng(seed).choice(NX * NY, sample_rays, replace=False)
     t0 = time.perf_counter()
-    g.render(oracle.camera(*camera_args()), BOX, 0.0, REL_TOL, mode=1, pix=pix,
+    g.render(oracle.camera(*camera_args()), DEPTH, 0.0, REL_TOL, mode=1, pix=pix,
              nthreads=nthreads)
     t_render = time.perf_counter() - t0
     t_full = t_fixed + t_render * (NX * NY) / sample_rays
@@ -175,6 +203,8 @@ def run_ours(args, rank, world, local_rank):
     n = cells.n
     ctx = ilc.Context(local_rank)
     ctx.load_gaunt()
+    if args.z_window is not None:
+        ctx.set_z_window(args.z_window)
     cam = ilc.camera(*camera_args())
     scaling = ilc.LosScaling(1.0, 1.0, ilc.DA_PIXEL_AREA)
     dev = torch.device("cuda", local_rank)
@@ -185,14 +215,16 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
 
     def step():
-        return ctx.project_xray_flux(d_cells, d_rho, d_u, d_xe, cam, BOX, rel_tol=REL_TOL,
+        return ctx.project_xray_flux(d_cells, d_rho, d_u, d_xe, cam, DEPTH, rel_tol=REL_TOL,
                                      controller=ilc.CONTROLLER_FP64, e_min=E_MIN, e_max=E_MAX,
                                      num_samples=NUM_SAMPLES, scaling=scaling, image=d_img)
 
-    for _ in range(args.warmup):
+    for i in range(max(args.warmup, 1)):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         step()
+        if i == 0:
+            tuned = tune_schedule(ctx, cam, args, torch.cuda.get_device_name(dev))
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -227,7 +259,7 @@ def run_ours(args, rank, world, local_rank):
 
     def e2e_step():
         return ctx.project_xray_flux(h_cells.numpy(), h_rho.numpy(), h_u.numpy(),
-                                     h_xe.numpy(), cam, BOX, rel_tol=REL_TOL,
+                                     h_xe.numpy(), cam, DEPTH, rel_tol=REL_TOL,
                                      controller=ilc.CONTROLLER_FP64, e_min=E_MIN, e_max=E_MAX,
                                      num_samples=NUM_SAMPLES, scaling=scaling,
                                      image=h_img.numpy())
@@ -266,9 +298,9 @@ def run_ours(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded NFW + uniform gas cells, numpy PCG64 seed 20171)",
-        "config": {"workload": f"xray_band_map_4M_cells_{NX}sq_rtol1e-3", "cells": n, "image": [NX, NY], "z_range_kpc": BOX,
+        "config": {"workload": f"xray_band_map_4M_cells_{NX}sq_rtol1e-3", "cells": n, "image": [NX, NY], "z_range_kpc": DEPTH, "camera_z": Z_START,
                    "rel_tol": REL_TOL, "controller": "fp64", "band_keV": [E_MIN, E_MAX],
-                   "parallelism": f"replicas x{world}",
+                   "parallelism": f"replicas x{world}", "schedule": tuned,
                    "l2": "flushed by a 256 MiB write before every step"},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(28 * n),
                 "d2h_bytes_per_step": int(4 * NX * NY)},
@@ -297,9 +329,17 @@ def main():
                     help="image side in pixels (1024 = the benchmark; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
+    ap.add_argument("--z-window", type=float, default=None,
+                    help="z window of the adaptive schedule in kpc (default: the tuned value)")
+    ap.add_argument("--z-start", type=float, default=0.0,
+                    help="camera plane position along z (profiling cases only)")
+    ap.add_argument("--z-range", type=float, default=None,
+                    help="integration depth in kpc (default: the 6 Mpc box; profiling only)")
     args = ap.parse_args()
-    global NX, NY
+    global NX, NY, Z_START, DEPTH
     NX = NY = args.image
+    Z_START = args.z_start
+    DEPTH = BOX if args.z_range is None else args.z_range
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

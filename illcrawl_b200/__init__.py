@@ -119,6 +119,23 @@ class Context:
     def set_step_limit(self, n):
         self.check(self.L.ilc_set_step_limit(self.h, int(n)))
 
+    def set_z_window(self, kpc):
+        self.check(self.L.ilc_set_z_window(self.h, float(kpc)))
+
+    def autotune_z_window(self, cam, z_range, rel_tol=1e-3, abs_tol=0.0,
+                          controller=CONTROLLER_FP64, candidates=(0, 2, 5, 10, 20, 40, 80),
+                          sample_stride=16):
+        """Times the adaptive render on a sample of tile rows for each candidate
+        z window, sets the fastest on the context; returns (best, {window: ms})."""
+        cand = np.ascontiguousarray(candidates, np.float32)
+        times = np.zeros(len(cand), np.float32)
+        best = ctypes.c_float(0.0)
+        self.check(self.L.ilc_autotune_z_window(self.h, ctypes.byref(cam), float(z_range),
+                                                Tolerance(abs_tol, rel_tol), controller,
+                                                _ptr(cand), len(cand), int(sample_stride),
+                                                ctypes.byref(best), _ptr(times)))
+        return float(best.value), {float(c): float(t) for c, t in zip(cand, times)}
+
     # ---- grid / nn8
     def setup_particles(self, xyzq):
         if not _is_dev(xyzq):

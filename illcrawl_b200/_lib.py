@@ -69,6 +69,7 @@ SIGNATURES = {
     "ilc_last_error": (ctypes.c_char_p, [_P]),
     "ilc_set_step_limit": (_int, [_P, _i64]),
     "ilc_get_stream": (_P, [_P]),
+    "ilc_set_z_window": (_int, [_P, _f32]),
     "ilc_nn8_setup_particles": (_int, [_P, _P, _u64, _int]),
     "ilc_grid_describe": (_int, [_P, _P]),
     "ilc_grid_export": (_int, [_P, _P, _P, _P, _int]),
@@ -86,6 +87,7 @@ SIGNATURES = {
     "ilc_project_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
                                      _f64, Tolerance, _i32, _P, _P, _int, _P]),
     "ilc_kernel_launches": (_u64, [_P]),
+    "ilc_autotune_z_window": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _i32, _i32, _P, _P]),
 }
 
 _lib = None

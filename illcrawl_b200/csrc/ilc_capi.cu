@@ -283,6 +283,14 @@ ilc_status ilc_set_step_limit(ilc_ctx* h, int64_t max_steps) {
 
 void* ilc_get_stream(ilc_ctx* h) { return h ? (void*)h->c.stream : nullptr; }
 
+ilc_status ilc_set_z_window(ilc_ctx* h, float z_window) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  if (!(z_window >= 0.0f) || !std::isfinite(z_window))
+    return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "z_window must be finite and >= 0");
+  h->c.z_window = z_window;
+  return ILC_OK;
+}
+
 ilc_status ilc_nn8_setup_particles(ilc_ctx* h, const float* particles, uint64_t n,
                                    int is_device) {
   if (!h) return ILC_ERR_INVALID_ARGUMENT;
@@ -553,5 +561,52 @@ ilc_status ilc_project_xray_flux(ilc_ctx* h, const float* cells, const float* rh
 }
 
 uint64_t ilc_kernel_launches(const ilc_ctx* h) { return h ? h->c.launches : 0; }
+
+ilc_status ilc_autotune_z_window(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                                 ilc_tolerance tol, int32_t controller, const float* candidates,
+                                 int32_t n_candidates, int32_t sample_stride, float* best,
+                                 float* times_ms) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "autotune before setup_particles");
+  if (!camera_ok(cam) || !candidates || n_candidates <= 0 || sample_stride <= 0 || !best ||
+      !(z_range > 0.0))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid autotune arguments");
+  RenderArgs a{};
+  camera_plane(*cam, a.cam);
+  a.nx = cam->num_pix_x;
+  a.ny = cam->num_pix_y;
+  a.z0 = 0.0f;
+  a.z_end = (float)z_range;
+  a.atol = tol.absolute;
+  a.rtol = tol.relative;
+  a.controller = controller;
+  a.apply_scale = false;
+  a.scale = 1.0f;
+  a.row_stride = sample_stride;
+  ILC_CUDA(c, c.out_b.ensure((size_t)a.nx * (size_t)a.ny * 4), "autotune image");
+  a.out = c.out_b.as<float>();
+  float best_ms = 0.0f;
+  for (int32_t i = 0; i < n_candidates; ++i) {
+    if (!(candidates[i] >= 0.0f) || !std::isfinite(candidates[i]))
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z window candidate");
+    a.window_override = candidates[i];
+    float ms = 0.0f;
+    ILC_CUDA(c, render_launch(c, a, &ms), "autotune render");
+    uint32_t flags = 0;
+    ilc_status st = read_flags(c, &flags, nullptr);
+    if (st) return st;
+    if (flags & FLAG_STEP_LIMIT)
+      return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the per-ray step limit");
+    if (times_ms) times_ms[i] = ms;
+    if (i == 0 || ms < best_ms) {
+      best_ms = ms;
+      *best = candidates[i];
+    }
+  }
+  c.z_window = *best;
+  return ILC_OK;
+}
 
 }  // extern "C"

@@ -50,6 +50,7 @@ struct Context {
   bool own_stream = false;
   std::string error;
   int64_t max_steps = 1 << 20;  // per-ray RKF step cap
+  float z_window = 0.0f;        // adaptive render: z window of the block schedule (0 = none)
 
   // particle grid
   bool has_grid = false;
@@ -125,6 +126,8 @@ struct RenderArgs {
   float scale;          // multiplier applied to each pixel
   bool apply_scale;
   float* out;           // device image
+  float window_override = -1.0f;  // >= 0: z window for this launch (autotuner)
+  int row_stride = 1;             // > 1: only every row_stride-th tile row (autotuner)
 };
 cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms);
 

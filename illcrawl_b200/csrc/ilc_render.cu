@@ -36,6 +36,8 @@ struct RenderK {
   int64_t fixed_steps;
   float fixed_h;
   int64_t max_steps;
+  float window;     // z window of the adaptive schedule (<= 0: none)
+  int row_stride;   // render every row_stride-th row of tiles (1 = all)
   float scale;
   int apply_scale;
   float* out;
@@ -45,10 +47,10 @@ struct RenderK {
 // 8 x 4 tile, so the 32 rays of a warp are spatial neighbours.
 constexpr int kRenderThreads = 128;
 constexpr int kTileX = 16, kTileY = 8;
-__device__ __forceinline__ void block_pixel(int& ix, int& iy) {
+__device__ __forceinline__ void block_pixel(int row_stride, int& ix, int& iy) {
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   ix = blockIdx.x * kTileX + (warp & 1) * 8 + (lane & 7);
-  iy = blockIdx.y * kTileY + (warp >> 1) * 4 + (lane >> 3);
+  iy = blockIdx.y * row_stride * kTileY + (warp >> 1) * 4 + (lane >> 3);
 }
 
 __global__ void __launch_bounds__(kRenderThreads)
@@ -57,18 +59,18 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
   __shared__ char4 spiral[1000];
   load_spiral(spiral, spiral_g);
   int ix, iy;
-  block_pixel(ix, iy);
+  block_pixel(a.row_stride, ix, iy);
   const bool active = ix < a.cam.nx && iy < a.cam.ny;
   WalkStats ws;
   unsigned long long steps = 0, acc = 0;
   bool at_limit = false;
-  if (active) {
-    float px, py, pz;
-    pixel_corner(a.cam, ix, iy, px, py, pz);
-    const float lx = a.cam.look0, ly = a.cam.look1, lz = a.cam.look2;
-    float I = 0.0f, z = a.z0, h = 1.0f, k1 = 0.0f;
-    float pts[4];
-    if (a.fixed_steps > 0) {
+  float px = 0.0f, py = 0.0f, pz = 0.0f;
+  if (active) pixel_corner(a.cam, ix, iy, px, py, pz);
+  const float lx = a.cam.look0, ly = a.cam.look1, lz = a.cam.look2;
+  float I = 0.0f, z = a.z0, h = 1.0f, k1 = 0.0f;
+  float pts[4];
+  if (a.fixed_steps > 0) {
+    if (active) {
       // Frozen uniform sequence: every step accepted, I += delta4.
       h = a.fixed_h;
       for (int64_t s = 0; s < a.fixed_steps; ++s) {
@@ -83,11 +85,19 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
         k1 = e[2];
       }
       steps = acc = (unsigned long long)a.fixed_steps;
-    } else {
-      rkf_points(z, h, pts);
-      const float fa = (float)a.atol, fr = (float)a.rtol;
-      while (z < a.z_end) {
-        if ((int64_t)steps >= a.max_steps) { at_limit = true; break; }
+    }
+  } else {
+    // Adaptive stepping, scheduled in z windows: every ray of the block runs
+    // its steps up to the window's end, then the block moves on together, so
+    // the rays in flight on an SM query one slab of the grid at a time. The
+    // windows only order the work; each ray's step sequence is unchanged.
+    rkf_points(z, h, pts);
+    const float fa = (float)a.atol, fr = (float)a.rtol;
+    bool run = active;
+    float wend = a.window > 0.0f ? a.z0 + a.window : a.z_end;
+    while (__syncthreads_or(run && z < a.z_end)) {
+      while (run && z < a.z_end && z < wend) {
+        if ((int64_t)steps >= a.max_steps) { at_limit = true; run = false; break; }
         float e[4];
         nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
         const float zb = z;
@@ -98,9 +108,10 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
         ++steps;
         if (z != zb) ++acc;
       }
+      wend = a.window > 0.0f ? wend + a.window : a.z_end;
     }
-    a.out[(size_t)iy * a.cam.nx + ix] = a.apply_scale ? I * a.scale : I;
   }
+  if (active) a.out[(size_t)iy * a.cam.nx + ix] = a.apply_scale ? I * a.scale : I;
   if (at_limit) atomicOr(flags, FLAG_STEP_LIMIT);
   // warp-aggregated statistics
   unsigned long long c = ws.cells, k = ws.cands, st = steps, ac = acc, mx = steps,
@@ -144,11 +155,14 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   k.fixed_steps = a.fixed_steps;
   k.fixed_h = a.fixed_h;
   k.max_steps = c.max_steps;
+  k.window = a.window_override >= 0.0f ? a.window_override : c.z_window;
+  k.row_stride = a.row_stride > 1 ? a.row_stride : 1;
   k.scale = a.scale;
   k.apply_scale = a.apply_scale ? 1 : 0;
   k.out = a.out;
   const GridView g = make_grid_view(c);
-  dim3 grid((a.nx + kTileX - 1) / kTileX, (a.ny + kTileY - 1) / kTileY);
+  const int tile_rows = (a.ny + kTileY - 1) / kTileY;
+  dim3 grid((a.nx + kTileX - 1) / kTileX, (tile_rows + k.row_stride - 1) / k.row_stride);
   if (!c.ev0) {
     if ((e = cudaEventCreate(&c.ev0)) || (e = cudaEventCreate(&c.ev1))) return e;
   }

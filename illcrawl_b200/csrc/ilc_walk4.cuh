@@ -12,11 +12,6 @@
 // reference's, bit for bit. What is shared is the spiral/cell bookkeeping and
 // the candidate loads (one 16-byte load serves four distance tests). Points in
 // a different cell or subcell are walked in a further pass.
-//
-// Distances for pairs of points are evaluated with sm_100's paired fp32
-// instructions (__fadd2_rn / __fmul2_rn): each lane of the pair is an IEEE
-// round-to-nearest add or multiply, so the results equal the scalar
-// (x*x + y*y) + z*z of the reference's op order.
 #pragma once
 
 #include "ilc_device.cuh"
@@ -103,10 +98,6 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
                                       Step4& s, unsigned mask, int cx, int cy, int cz, int sub,
                                       WalkStats& st) {
   const char4* order = spiral + sub * 125;
-  const float2 nqx01 = make_float2(-s.qx[0], -s.qx[1]), nqx23 = make_float2(-s.qx[2], -s.qx[3]);
-  const float2 nqy01 = make_float2(-s.qy[0], -s.qy[1]), nqy23 = make_float2(-s.qy[2], -s.qy[3]);
-  const float2 nqz01 = make_float2(-s.qz[0], -s.qz[1]), nqz23 = make_float2(-s.qz[2], -s.qz[3]);
-  const float2 crad = make_float2(g.cell_radius, g.cell_radius);
   unsigned act = mask;
   for (int it = 0; it < 125; ++it) {
     const char4 o = order[it];
@@ -116,19 +107,13 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     const float ccz = (g.min2 + (float)iz * g.cs2) + g.half2;
     {
       // early break per point: |c - q|^2 > (R + cell_radius)^2
-      const float2 cx2 = make_float2(ccx, ccx), cy2 = make_float2(ccy, ccy),
-                   cz2 = make_float2(ccz, ccz);
-      float2 ex = __fadd2_rn(cx2, nqx01), ey = __fadd2_rn(cy2, nqy01), ez = __fadd2_rn(cz2, nqz01);
-      const float2 dd01 = __fadd2_rn(__fadd2_rn(__fmul2_rn(ex, ex), __fmul2_rn(ey, ey)),
-                                     __fmul2_rn(ez, ez));
-      ex = __fadd2_rn(cx2, nqx23); ey = __fadd2_rn(cy2, nqy23); ez = __fadd2_rn(cz2, nqz23);
-      const float2 dd23 = __fadd2_rn(__fadd2_rn(__fmul2_rn(ex, ex), __fmul2_rn(ey, ey)),
-                                     __fmul2_rn(ez, ez));
-      const float2 r01 = __fadd2_rn(make_float2(s.R[0], s.R[1]), crad);
-      const float2 r23 = __fadd2_rn(make_float2(s.R[2], s.R[3]), crad);
-      const float2 rr01 = __fmul2_rn(r01, r01), rr23 = __fmul2_rn(r23, r23);
-      unsigned brk = (dd01.x > rr01.x ? 1u : 0u) | (dd01.y > rr01.y ? 2u : 0u) |
-                     (dd23.x > rr23.x ? 4u : 0u) | (dd23.y > rr23.y ? 8u : 0u);
+      unsigned brk = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float ex = ccx - s.qx[j], ey = ccy - s.qy[j], ez = ccz - s.qz[j];
+        const float r = s.R[j] + g.cell_radius;
+        if ((ex * ex + ey * ey) + ez * ez > r * r) brk |= 1u << j;
+      }
       act &= ~brk;
     }
     if (!act) break;
@@ -143,18 +128,16 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     st.cands += na * (uint32_t)max(be.y - be.x, 0);
     for (int p = be.x; p < be.y; ++p) {
       const float4 P = __ldg(&g.parts[p]);
-      const float2 px = make_float2(P.x, P.x), py = make_float2(P.y, P.y),
-                   pz = make_float2(P.z, P.z);
-      float2 fx = __fadd2_rn(px, nqx01), fy = __fadd2_rn(py, nqy01), fz = __fadd2_rn(pz, nqz01);
-      const float2 d01 = __fadd2_rn(__fadd2_rn(__fmul2_rn(fx, fx), __fmul2_rn(fy, fy)),
-                                    __fmul2_rn(fz, fz));
-      fx = __fadd2_rn(px, nqx23); fy = __fadd2_rn(py, nqy23); fz = __fadd2_rn(pz, nqz23);
-      const float2 d23 = __fadd2_rn(__fadd2_rn(__fmul2_rn(fx, fx), __fmul2_rn(fy, fy)),
-                                    __fmul2_rn(fz, fz));
-      s4_test<0>(s, act, d01.x, P.w);
-      s4_test<1>(s, act, d01.y, P.w);
-      s4_test<2>(s, act, d23.x, P.w);
-      s4_test<3>(s, act, d23.y, P.w);
+      float d2[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float fx = P.x - s.qx[j], fy = P.y - s.qy[j], fz = P.z - s.qz[j];
+        d2[j] = (fx * fx + fy * fy) + fz * fz;
+      }
+      s4_test<0>(s, act, d2[0], P.w);
+      s4_test<1>(s, act, d2[1], P.w);
+      s4_test<2>(s, act, d2[2], P.w);
+      s4_test<3>(s, act, d2[3], P.w);
     }
   }
 }

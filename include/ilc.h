@@ -105,6 +105,10 @@ const char* ilc_last_error(const ilc_ctx* ctx);
 ilc_status ilc_set_step_limit(ilc_ctx* ctx, int64_t max_steps);
 /* The context's cudaStream_t, for callers that time or order work around it. */
 void* ilc_get_stream(ilc_ctx* ctx);
+/* Schedule of the adaptive render: rays of a thread block advance through
+ * z_window-thick slabs together (0 = every ray runs to its end independently).
+ * Changes the order of work only, never a result. */
+ilc_status ilc_set_z_window(ilc_ctx* ctx, float z_window);
 
 /* ---- particle grid + nn8 backend ------------------------------------------
  * ilc_nn8_setup_particles replaces reconstruction_backend::setup_particles
@@ -208,6 +212,17 @@ ilc_status ilc_project_xray_flux(ilc_ctx* ctx, const float* cells, const float* 
                                  ilc_tolerance tol, int32_t controller,
                                  const ilc_los_scaling* scaling, float* image, int is_device,
                                  ilc_render_stats* stats);
+
+/* Autotuner of the adaptive render's schedule: renders every sample_stride-th
+ * row of 8-pixel tiles of the view once per candidate z window, times the
+ * render kernel with CUDA events, sets the fastest on the context and returns
+ * it in *best (times_ms, may be NULL: n_candidates kernel times). Needs the
+ * particles set up. The result depends on the particle distribution and the
+ * view, so callers cache it per workload. */
+ilc_status ilc_autotune_z_window(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                                 ilc_tolerance tol, int32_t controller, const float* candidates,
+                                 int32_t n_candidates, int32_t sample_stride, float* best,
+                                 float* times_ms);
 
 /* Number of kernels this context has launched so far. */
 uint64_t ilc_kernel_launches(const ilc_ctx* ctx);
