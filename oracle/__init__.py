@@ -54,7 +54,7 @@ def _declare(L):
     L.orc_render_fixed.argtypes = [P, P, f64, i64, ctypes.c_int, P, i64, P, P, ctypes.c_int]
     L.orc_render_record.argtypes = [P, P, f64, f64, f64, ctypes.c_int, i64, P, i64, P, P, i64,
                                     P, ctypes.c_int]
-    L.orc_render_replay.argtypes = [P, P, P, i64, P, i64, P, ctypes.c_int, P, ctypes.c_int]
+    L.orc_render_replay.argtypes = [P, P, P, i64, P, i64, P, ctypes.c_int, P, P, ctypes.c_int]
     L.orc_los_scale.argtypes = [P, f64, f64, f64, ctypes.c_int]; L.orc_los_scale.restype = f32
     L.orc_gaunt_lookup.argtypes = [P, ctypes.c_int, ctypes.c_int, f32, f32]
     L.orc_gaunt_lookup.restype = f32
@@ -168,9 +168,10 @@ class Grid:
         pixa = None if pix is None else np.ascontiguousarray(pix, np.int64)
         n = np.ascontiguousarray(n, np.int32)
         out = np.zeros(npix, np.float32)
+        out_d = np.zeros(npix, np.float64) if precision == 1 else None
         lib().orc_render_replay(self.h, ctypes.byref(cam), _p(pixa), npix, _p(hs), hs.shape[1],
-                                _p(n), precision, _p(out), nthreads)
-        return out
+                                _p(n), precision, _p(out), _p(out_d), nthreads)
+        return out if out_d is None else out_d
 
 
 def camera_setup(cam):
@@ -237,3 +238,46 @@ def nn8_lists(grid, pts, merge=False, lists=None, nthreads=0):
     L.orc_nn8_query_lists(grid.h, _p(pts), n, int(merge), _p(ld), _p(lv), _p(li), _p(out),
                           nthreads)
     return out, (ld, lv, li)
+
+
+def _declare_adjoint(L):
+    P, i64 = ctypes.c_void_p, ctypes.c_int64
+    L.orc_xray_band_grad.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, i64, ctypes.c_float,
+                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                     ctypes.c_int, P, P, P, ctypes.c_int]
+    L.orc_adjoint.argtypes = [P, P, P, i64, P, i64, P, P, ctypes.c_int, P, ctypes.c_int]
+
+
+def _adj_lib():
+    L = lib()
+    if not getattr(L, "_adj_declared", False):
+        _declare_adjoint(L)
+        L._adj_declared = True
+    return L
+
+
+def xray_band_grad(table, rho, u, xe, z, dL, Emin, Emax, num_samples, precision=0, nthreads=0):
+    """Per-cell band flux q, dq/dlnT and dq/dlnrho (exact derivatives of the
+    adaptive energy integration)."""
+    t = np.ascontiguousarray(table, np.float32)
+    rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+    q = np.zeros_like(rho)
+    dq = np.zeros(rho.shape, np.float64)
+    dqr = np.zeros(rho.shape, np.float64)
+    _adj_lib().orc_xray_band_grad(_p(t), t.shape[1], t.shape[0], _p(rho), _p(u), _p(xe),
+                                  rho.size, z, dL, Emin, Emax, num_samples, precision, _p(q),
+                                  _p(dq), _p(dqr), nthreads)
+    return q, dq, dqr
+
+
+def adjoint(grid, cam, hs, n, gI, pix=None, precision=1, nthreads=0):
+    """sum_k gI[k] * dI_k/dq over frozen step sequences; float64 array in the
+    original particle order."""
+    hs = np.ascontiguousarray(hs, np.float32)
+    n = np.ascontiguousarray(n, np.int32)
+    gI = np.ascontiguousarray(gI, np.float64)
+    pixa = None if pix is None else np.ascontiguousarray(pix, np.int64)
+    grad = np.zeros(grid.xyzq.shape[0], np.float64)
+    _adj_lib().orc_adjoint(grid.h, ctypes.byref(cam), _p(pixa), hs.shape[0], _p(hs), hs.shape[1],
+                           _p(n), _p(gI), precision, _p(grad), nthreads)
+    return grad

@@ -743,6 +743,181 @@ static inline R band_flux(const Gaunt& G, R Emin, R Emax, R reltol, R T, R xe, R
   return em;
 }
 
+// ---- derivatives for the adjoint -------------------------------------------
+// Partial derivatives of the spectral emission (dE = 1) at fixed rho, xe:
+//   with Tinv = 1000/(kB T), texel coordinates u = (ln(Ryd/(kB T)) - x0)/dx and
+//   v = (ln(1e3 E/(kB T)) - y0)/dy, base = A T^-1/2 exp(-E Tinv) / r^2:
+//   d/dlnT = base * (g * (E Tinv - 1/2) - (g_u/dx + g_v/dy))
+//   d/dE   = base * (-g Tinv + g_v / (dy E))
+// g_u, g_v: partial derivatives of the bilinear blend inside the texel.
+template <class R>
+static inline void gaunt_grad_uv(const Gaunt& G, R u, R v, R* gu, R* gv) {
+  typedef mathf<R> M;
+  *gu = *gv = (R)0;
+  if (!(u == u) || !(v == v)) return;
+  u = std::min(std::max(u, (R)-4), (R)(G.w + 4));
+  v = std::min(std::max(v, (R)-4), (R)(G.h + 4));
+  const R us = u - (R)0.5, vs = v - (R)0.5;
+  const R fu = M::floor(us), fv = M::floor(vs);
+  const int i0 = (int)fu, j0 = (int)fv;
+  const R a = us - fu, b = vs - fv;
+  const R t00 = texel<R>(G, i0, j0), t10 = texel<R>(G, i0 + 1, j0);
+  const R t01 = texel<R>(G, i0, j0 + 1), t11 = texel<R>(G, i0 + 1, j0 + 1);
+  *gu = ((R)1 - b) * (t10 - t00) + b * (t11 - t01);
+  *gv = ((R)1 - a) * (t01 - t00) + a * (t11 - t10);
+}
+
+// value (the forward's own expression) and its lnT / E partials (double).
+template <class R>
+static inline void brems_partials(const Gaunt& G, R E, R T, R xe, R rho, R r, R* val,
+                                  double* d_lnT, double* d_E) {
+  typedef XC<R> C;
+  *val = brems<R>(G, E, (R)1, T, xe, rho, r);
+  const double Ed = (double)E, Td = (double)T;
+  const double kB = (double)C::kB();
+  const double ion = (double)C::nconv() * (double)rho * (double)xe;
+  const double Tinv = 1000.0 / (kB * Td);
+  const double ux = (std::log((double)C::Ryd() / (kB * Td)) - (double)G.x0) / (double)G.dx;
+  const double vy = (std::log((double)C::kilo() * Ed / (kB * Td)) - (double)G.y0) / (double)G.dy;
+  const double g = gaunt_sample<double>(G, ux, vy);
+  double gu, gv;
+  gaunt_grad_uv<double>(G, ux, vy, &gu, &gv);
+  const double base = (double)C::pref() * ion * ion / std::sqrt(Td) * std::exp(-Ed * Tinv) /
+                      ((double)r * (double)r);
+  *d_lnT = base * (g * (Ed * Tinv - 0.5) - (gu / (double)G.dx + gv / (double)G.dy));
+  *d_E = base * (-g * Tinv + gv / ((double)G.dy * Ed));
+}
+
+static inline double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+
+// integrate_spectral_flux(XRAY_FLUX) in forward mode: the values follow the
+// forward exactly (same ops, same decisions), and every state variable carries
+// its derivative with respect to ln T, through the step controller as well
+// (the energy steps are adaptive, so they move with T): the sqrt-sqrt factor,
+// the clamps (derivative 0 when clamped) and the final-step adjustment.
+// which = 0: tangent along ln T; which = 1: along ln rho (brems ~ rho^2, so its
+// partial is 2*brems; the energy steps still move with rho through the error
+// estimate when the absolute tolerance dominates).
+template <class R>
+static inline void band_flux_tangent(const Gaunt& G, R Emin, R Emax, R reltol, R T, R xe, R rho,
+                                     R dL, int which, R* q, double* dq) {
+  const R atol = reltol, rtol = (R)1, eps = (R)0, hmin = (R)1.e-3f, hmax = (R)100;
+  R I = (R)0, z = Emin, h = (Emax - Emin) * reltol, k1;
+  double dI = 0, dz = 0, dh = 0, dk1, dkE;
+  const R end = Emax;
+  brems_partials<R>(G, z, T, xe, rho, dL, &k1, &dk1, &dkE);
+  if (which == 1) dk1 = 2.0 * (double)k1;
+  R p[4];
+  double dp[4] = {0, 0, 0, 0};
+  rkf_points<R>(z, h, p);
+  const double c[4] = {3. / 8., 12. / 13., 1.0, 0.5};
+  int guard = 0;
+  while (z < end && guard < 100000) {
+    R e[4];
+    double de[4];
+    for (int j = 0; j < 4; ++j) {
+      double pl, pe;
+      brems_partials<R>(G, p[j], T, xe, rho, dL, &e[j], &pl, &pe);
+      if (which == 1) pl = 2.0 * (double)e[j];
+      de[j] = pl + pe * dp[j];
+    }
+    // rkf_advance_ref with tangents
+    R b4 = (R)25 / (R)216 * k1 + (R)1408 / (R)2565 * e[0] + (R)2197 / (R)4101 * e[1] -
+           (R)1 / (R)5 * e[2];
+    R b5 = (R)16 / (R)135 * k1 + (R)6656 / (R)12825 * e[0] + (R)28561 / (R)56430 * e[1] -
+           (R)9 / (R)50 * e[2] + (R)2 / (R)55 * e[3];
+    const double db4 = 25. / 216. * dk1 + 1408. / 2565. * de[0] + 2197. / 4101. * de[1] -
+                       1. / 5. * de[2];
+    const double db5 = 16. / 135. * dk1 + 6656. / 12825. * de[0] + 28561. / 56430. * de[1] -
+                       9. / 50. * de[2] + 2. / 55. * de[3];
+    const double dd4 = db4 * (double)h + (double)b4 * dh;
+    const double dd5 = db5 * (double)h + (double)b5 * dh;
+    const R d4 = b4 * h, d5 = b5 * h;
+    const R est4 = I + d4;
+    const double dest4 = dI + dd4;
+    const R old = z;
+    const double dold = dz;
+    z += h;
+    dz += dh;
+    R s = (R)2;
+    double ds = 0;
+    if (d4 != d5) {
+      const R err = mathf<R>::fabs(d5 - d4);
+      const double derr = sgn((double)d5 - (double)d4) * (dd5 - dd4);
+      const R ratio = I / z * rtol;
+      const R srt = mathf<R>::fabs(ratio);
+      const double dsrt = sgn((double)ratio) * (double)rtol *
+                          (dI / (double)z - (double)I * dz / ((double)z * (double)z));
+      const R ot = mathf<R>::fmax(atol, srt);
+      const double dot_ = srt > atol ? dsrt : 0.0;
+      s = mathf<R>::sqrt(mathf<R>::sqrt(ot * h / ((R)2 * err)));
+      ds = (double)s * 0.25 * (dot_ / (double)ot + dh / (double)h - derr / (double)err);
+    }
+    R nh = s * h;
+    double dnh = ds * (double)h + (double)s * dh;
+    if (nh < hmin) { nh = hmin; dnh = 0; }
+    else if (nh > hmax) { nh = hmax; dnh = 0; }
+    s = nh / h;
+    if (s < (R)0.95) {
+      z = old;
+      dz = dold;
+    } else {
+      I = est4;
+      dI = dest4;
+      k1 = e[2];
+      dk1 = de[2];
+    }
+    h = nh;
+    dh = dnh;
+    if (z + h >= end) { h = end - z + eps; dh = -dz; }
+    rkf_points<R>(z, h, p);
+    for (int j = 0; j < 4; ++j) dp[j] = dz + c[j] * dh;
+    ++guard;
+  }
+  *q = I;
+  *dq = dI;
+}
+
+// Adjoint of one ray over its frozen accepted steps: every accepted step adds
+// h*(25/216 k1 + 1408/2565 e0 + 2197/4101 e1 - 1/5 e2) to I, k1 being the
+// previous step's e2 (0 before the first step), and each e is the finalize
+// of its 8 slots, sum(w v)/sum(w) -> d e / d v_p = w_p / sum(w).
+template <class R>
+static void adjoint_ray(const Grid& g, const RayGeom<R>& rg, R z0, const float* hs,
+                        int64_t nsteps, R gI, double* grad) {
+  R z = z0;
+  Slots<R> prev;
+  bool have_prev = false;
+  for (int64_t i = 0; i < nsteps; ++i) {
+    const R h = (R)hs[i];
+    R p[4];
+    rkf_points<R>(z, h, p);
+    const R coef[3] = {h * (R)1408 / (R)2565, h * (R)2197 / (R)4101, -h / (R)5};
+    Slots<R> s[3];
+    for (int j = 0; j < 3; ++j) {
+      slots_init(s[j]);
+      nn8_search<R>(g, rg.pix[0] + p[j] * rg.look[0], rg.pix[1] + p[j] * rg.look[1],
+                    rg.pix[2] + p[j] * rg.look[2], s[j], nullptr);
+    }
+    auto scatter = [&](const Slots<R>& sl, R c) {
+      R w[8], ws = (R)0;
+      for (int t = 0; t < 8; ++t) { w[t] = weight3d(sl.d[t]); ws += w[t]; }
+      if (ws == (R)0 || !(ws == ws)) return;
+      for (int t = 0; t < 8; ++t) {
+        if (sl.id[t] < 0 || w[t] == (R)0) continue;
+        const double add = (double)(gI * c * (w[t] / ws));
+#pragma omp atomic
+        grad[sl.id[t]] += add;
+      }
+    };
+    for (int j = 0; j < 3; ++j) scatter(s[j], coef[j]);
+    if (have_prev) scatter(prev, h * (R)25 / (R)216);
+    prev = s[2];
+    have_prev = true;
+    z += h;
+  }
+}
+
 }  // namespace orc
 
 // ==========================================================================
@@ -990,7 +1165,7 @@ int orc_render_record(void* h, const orc_camera* c, double z_range, double atol,
 // Frozen replay of given per-ray step sequences (hs: npix x cap, counts n).
 int orc_render_replay(void* h, const orc_camera* c, const int64_t* pix, int64_t npix,
                       const float* hs, int64_t cap, const int32_t* n, int precision, float* out,
-                      int nthreads) {
+                      double* out_d, int nthreads) {
   Grid* g = (Grid*)h;
   Camera cam;
   std::memcpy(&cam, c, sizeof(Camera));
@@ -1008,7 +1183,9 @@ int orc_render_replay(void* h, const orc_camera* c, const int64_t* pix, int64_t 
     } else {
       RayGeom<double> rg;
       ray_geom_d(d, ix, iy, rg);
-      out[k] = (float)replay_ray<double>(*g, rg, 0.0, hs + k * cap, n[k], nullptr);
+      const double v = replay_ray<double>(*g, rg, 0.0, hs + k * cap, n[k], nullptr);
+      out[k] = (float)v;
+      if (out_d) out_d[k] = v;
     }
   }
   return 0;
@@ -1068,6 +1245,73 @@ int orc_xray_band(const float* table, int w, int hgt, const float* rho, const fl
                                         1. / (double)num_samples, T, xe[i], rho[i], dL);
     }
   }
+  return 0;
+}
+
+// xray_flux and its derivatives with respect to ln T and ln rho (forward mode
+// through the adaptive energy integration).
+int orc_xray_band_grad(const float* table, int w, int hgt, const float* rho, const float* u,
+                       const float* xe, int64_t n, float z, float dL, float Emin, float Emax,
+                       int num_samples, int precision, float* q_out, double* dq_out,
+                       double* dqr_out, int nthreads) {
+  Gaunt G = make_gaunt(table, w, hgt);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    if (precision == 0) {
+      const float T = temperature<float>(u[i], xe[i]);
+      float q;
+      double dq, dqr;
+      band_flux_tangent<float>(G, (1.f + z) * Emin, (1.f + z) * Emax, 1.f / (float)num_samples,
+                               T, xe[i], rho[i], dL, 0, &q, &dq);
+      band_flux_tangent<float>(G, (1.f + z) * Emin, (1.f + z) * Emax, 1.f / (float)num_samples,
+                               T, xe[i], rho[i], dL, 1, &q, &dqr);
+      q_out[i] = q;
+      dq_out[i] = dq;
+      dqr_out[i] = dqr;
+    } else {
+      const double T = temperature<double>(u[i], xe[i]);
+      double q, dq, dqr;
+      band_flux_tangent<double>(G, (1. + z) * Emin, (1. + z) * Emax, 1. / (double)num_samples,
+                                T, xe[i], rho[i], dL, 0, &q, &dq);
+      band_flux_tangent<double>(G, (1. + z) * Emin, (1. + z) * Emax, 1. / (double)num_samples,
+                                T, xe[i], rho[i], dL, 1, &q, &dqr);
+      q_out[i] = (float)q;
+      dq_out[i] = dq;
+      dqr_out[i] = dqr;
+    }
+  }
+  return 0;
+}
+
+// Adjoint over frozen per-ray step sequences (hs: npix x cap, counts n): adds
+// gI[k] * dI_k/dq_p into grad (n_particles, ORIGINAL particle order).
+int orc_adjoint(void* h, const orc_camera* c, const int64_t* pix, int64_t npix, const float* hs,
+                int64_t cap, const int32_t* n, const double* gI, int precision, double* grad,
+                int nthreads) {
+  Grid* g = (Grid*)h;
+  Camera cam;
+  std::memcpy(&cam, c, sizeof(Camera));
+  CamDev d;
+  camera_setup(cam, &d);
+  const size_t np = g->s2u.size();
+  std::vector<double> gs(np, 0.0);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t k = 0; k < npix; ++k) {
+    const int64_t p = pix ? pix[k] : k;
+    const int ix = (int)(p % cam.nx), iy = (int)(p / cam.nx);
+    if (precision == 0) {
+      RayGeom<float> rg;
+      ray_geom_f(d, ix, iy, rg);
+      adjoint_ray<float>(*g, rg, 0.0f, hs + k * cap, n[k], (float)gI[k], gs.data());
+    } else {
+      RayGeom<double> rg;
+      ray_geom_d(d, ix, iy, rg);
+      adjoint_ray<double>(*g, rg, 0.0, hs + k * cap, n[k], gI[k], gs.data());
+    }
+  }
+  for (size_t i = 0; i < np; ++i) grad[g->s2u[i]] += gs[i];
   return 0;
 }
 
