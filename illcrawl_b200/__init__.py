@@ -259,6 +259,29 @@ class Context:
             Tolerance(abs_tol, rel_tol), controller, sc, _ptr(image), dev, ctypes.byref(st)))
         return image, st.as_dict()
 
+    def adjoint_xray_flux(self, cells, rho, u, xe, cam, z_range, target, mode=0, rel_tol=1e-3,
+                          abs_tol=0.0, controller=CONTROLLER_FP64, redshift=REDSHIFT,
+                          luminosity_distance=LUMINOSITY_DISTANCE, e_min=0.5, e_max=7.0,
+                          num_samples=100, scaling=None):
+        """Band map + gradient of sum (log I - log target)^2 with respect to
+        per-cell ln rho and ln T (ilc_adjoint_xray_flux). Host arrays in,
+        host arrays out. mode: 0 checkpoint, 1 recompute."""
+        cells = np.ascontiguousarray(cells, np.float32).reshape(-1, 4)
+        rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+        target = np.ascontiguousarray(target, np.float32)
+        n = u.shape[0]
+        img = np.zeros((cam.num_pix_y, cam.num_pix_x), np.float32)
+        g_r = np.zeros(n, np.float32)
+        g_t = np.zeros(n, np.float32)
+        st = _lib.AdjointStats()
+        sc = None if scaling is None else ctypes.byref(scaling)
+        self.check(self.L.ilc_adjoint_xray_flux(
+            self.h, _ptr(cells), _ptr(rho), _ptr(u), _ptr(xe), n, redshift, luminosity_distance,
+            e_min, e_max, num_samples, ctypes.byref(cam), float(z_range),
+            Tolerance(abs_tol, rel_tol), controller, sc, _ptr(target), int(mode), _ptr(img),
+            _ptr(g_r), _ptr(g_t), 0, ctypes.byref(st)))
+        return img, g_r, g_t, st.as_dict()
+
     @property
     def kernel_launches(self):
         return int(self.L.ilc_kernel_launches(self.h))

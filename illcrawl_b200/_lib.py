@@ -58,6 +58,17 @@ class RenderStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class AdjointStats(ctypes.Structure):
+    _fields_ = [("loss", ctypes.c_double), ("quantity_ms", ctypes.c_float),
+                ("forward_ms", ctypes.c_float), ("adjoint_ms", ctypes.c_float),
+                ("forward_steps", ctypes.c_uint64), ("adjoint_steps", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+ADJOINT_CHECKPOINT, ADJOINT_RECOMPUTE = 0, 1
+
 _P = ctypes.c_void_p
 _u64, _i64, _i32, _f32, _f64, _int = (ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,
                                       ctypes.c_float, ctypes.c_double, ctypes.c_int)
@@ -88,6 +99,8 @@ SIGNATURES = {
                                      _f64, Tolerance, _i32, _P, _P, _int, _P]),
     "ilc_kernel_launches": (_u64, [_P]),
     "ilc_autotune_z_window": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _i32, _i32, _P, _P]),
+    "ilc_adjoint_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
+                                     _f64, Tolerance, _i32, _P, _P, _i32, _P, _P, _P, _int, _P]),
 }
 
 _lib = None

@@ -167,6 +167,28 @@ ilc_status read_flags(Context& c, uint32_t* flags, DevStats* stats) {
   return ILC_OK;
 }
 
+// Grid over the n float4 particles already in c.tmp_in (setup_particles).
+ilc_status build_grid_staged(Context& c, uint64_t n) {
+  c.has_grid = false;
+  float mn[3], mx[3];
+  bool nonfinite = false;
+  ILC_CUDA(c, grid_bbox(c, c.tmp_in.as<float4>(), n, mn, mx, &nonfinite), "bounding box");
+  if (nonfinite) return fail(c, ILC_ERR_NONFINITE_INPUT, "non-finite particle coordinates");
+  GridParams g;
+  make_grid_params(mn, mx, n, &g);
+  if (g.total >= (1ull << 32) || g.n[0] <= 0 || g.n[1] <= 0 || g.n[2] <= 0)
+    return fail(c, ILC_ERR_GRID_TOO_LARGE, "grid has more than 2^32 cells");
+  c.gp = g;
+  ILC_CUDA(c, grid_build_device(c, c.tmp_in.as<float4>(), n), "grid build");
+  uint32_t flags = 0;
+  ilc_status st = read_flags(c, &flags, nullptr);
+  if (st) return st;
+  if (flags & FLAG_KEY_RANGE) return fail(c, ILC_ERR_INTERNAL, "particle outside its grid");
+  c.n_particles = n;
+  c.has_grid = true;
+  return ILC_OK;
+}
+
 ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_tolerance tol,
                          int32_t controller, int64_t fixed_steps,
                          const ilc_los_scaling* scaling, float* image, int is_device,
@@ -264,7 +286,9 @@ void ilc_destroy(ilc_ctx* h) {
   if (c.stream) cudaStreamSynchronize(c.stream);
   for (DevBuf* b : {&c.parts, &c.cells, &c.s2u, &c.keys_a, &c.keys_b, &c.vals_a, &c.vals_b,
                     &c.hist, &c.tmp_in, &c.gaunt, &c.list_d, &c.list_v, &c.list_id, &c.in_a,
-                    &c.in_b, &c.in_c, &c.out_a, &c.out_b, &c.out_c, &c.spiral, &c.flags})
+                    &c.in_b, &c.in_c, &c.out_a, &c.out_b, &c.out_c, &c.spiral, &c.flags,
+                    &c.rec_h, &c.rec_n, &c.adj_dT, &c.adj_dR, &c.adj_grad, &c.adj_seed,
+                    &c.adj_loss})
     b->release();
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
@@ -539,28 +563,142 @@ ilc_status ilc_project_xray_flux(ilc_ctx* h, const float* cells, const float* rh
   ILC_CUDA(c, quantity_xray_flux_launch(c, a, b, d, n, redshift, luminosity_distance, e_min,
                                         e_max, num_samples, c.tmp_in.as<float>() + 3, 4),
            "xray_flux kernel");
-  c.has_grid = false;
-  float mn[3], mx[3];
-  bool nonfinite = false;
-  ILC_CUDA(c, grid_bbox(c, c.tmp_in.as<float4>(), n, mn, mx, &nonfinite), "bounding box");
-  if (nonfinite) return fail(c, ILC_ERR_NONFINITE_INPUT, "non-finite particle coordinates");
-  GridParams g;
-  make_grid_params(mn, mx, n, &g);
-  if (g.total >= (1ull << 32) || g.n[0] <= 0 || g.n[1] <= 0 || g.n[2] <= 0)
-    return fail(c, ILC_ERR_GRID_TOO_LARGE, "grid has more than 2^32 cells");
-  c.gp = g;
-  ILC_CUDA(c, grid_build_device(c, c.tmp_in.as<float4>(), n), "grid build");
-  uint32_t flags = 0;
-  st = read_flags(c, &flags, nullptr);
+  st = build_grid_staged(c, n);
   if (st) return st;
-  if (flags & FLAG_KEY_RANGE) return fail(c, ILC_ERR_INTERNAL, "particle outside its grid");
-  c.n_particles = n;
-  c.has_grid = true;
-  c.list_n = 0;
   return render_common(c, cam, z_range, tol, controller, 0, scaling, image, is_device, stats);
 }
 
 uint64_t ilc_kernel_launches(const ilc_ctx* h) { return h ? h->c.launches : 0; }
+
+ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rho,
+                                 const float* u, const float* xe, uint64_t n, float redshift,
+                                 float luminosity_distance, float e_min, float e_max,
+                                 int32_t num_samples, const ilc_camera* cam, double z_range,
+                                 ilc_tolerance tol, int32_t controller,
+                                 const ilc_los_scaling* scaling, const float* target, int32_t mode,
+                                 float* image, float* dL_dlnrho, float* dL_dlnT, int is_device,
+                                 ilc_adjoint_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (!cells || !rho || !u || !xe || !target || !image || !dL_dlnrho || !dL_dlnT || n == 0 ||
+      num_samples <= 0 || !(e_max >= e_min) || !camera_ok(cam) || !(z_range > 0.0) ||
+      !std::isfinite(z_range))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid adjoint arguments");
+  if (mode != ILC_ADJOINT_CHECKPOINT && mode != ILC_ADJOINT_RECOMPUTE)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "unknown adjoint mode");
+  if (controller != ILC_CONTROLLER_REF32 && controller != ILC_CONTROLLER_FP64)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "unknown controller");
+  if (!(tol.absolute >= 0.0) || !(tol.relative >= 0.0) ||
+      (tol.absolute <= 0.0 && tol.relative <= 0.0))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT,
+                "either the absolute or the relative tolerance has to be > 0");
+  if (n >= (1ull << 31)) return fail(c, ILC_ERR_GRID_TOO_LARGE, "more than 2^31 particles");
+  const int64_t npix = (int64_t)cam->num_pix_x * cam->num_pix_y;
+  cudaEvent_t q0, q1;
+  ILC_CUDA(c, cudaEventCreate(&q0), "event");
+  ILC_CUDA(c, cudaEventCreate(&q1), "event");
+  // 1. per-cell q (into the particles' q slot), dq/dln T, dq/dln rho
+  ILC_CUDA(c, c.tmp_in.ensure(n * 16), "particle staging");
+  ILC_CUDA(c, cudaMemcpyAsync(c.tmp_in.p, cells, n * 16,
+                              is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                              c.stream),
+           "cells copy");
+  const float *a, *b, *d;
+  ilc_status st = quantity_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  ILC_CUDA(c, c.adj_dT.ensure(n * 4), "dq/dlnT");
+  ILC_CUDA(c, c.adj_dR.ensure(n * 4), "dq/dlnrho");
+  cudaEventRecord(q0, c.stream);
+  ILC_CUDA(c, adjoint_cell_launch(c, a, b, d, n, redshift, luminosity_distance, e_min, e_max,
+                                  num_samples, c.tmp_in.as<float>() + 3, 4, c.adj_dT.as<float>(),
+                                  c.adj_dR.as<float>()),
+           "xray_flux derivative kernel");
+  cudaEventRecord(q1, c.stream);
+  // 2. grid
+  st = build_grid_staged(c, n);
+  if (st) return st;
+  // 3. forward render, recording the accepted steps in CHECKPOINT mode
+  RenderArgs ra{};
+  camera_plane(*cam, ra.cam);
+  ra.nx = cam->num_pix_x;
+  ra.ny = cam->num_pix_y;
+  ra.z0 = 0.0f;
+  ra.z_end = (float)z_range;
+  ra.atol = tol.absolute;
+  ra.rtol = tol.relative;
+  ra.controller = controller;
+  ra.apply_scale = scaling != nullptr;
+  ra.scale = scaling ? los_scale(*cam, z_range, *scaling) : 1.0f;
+  ILC_CUDA(c, c.out_b.ensure((size_t)npix * 4), "image");
+  ra.out = c.out_b.as<float>();
+  if (mode == ILC_ADJOINT_CHECKPOINT) {
+    ra.rec_cap = (int64_t)std::ceil(z_range / 0.2) + 2;
+    ILC_CUDA(c, c.rec_h.ensure((size_t)npix * (size_t)ra.rec_cap * 4),
+             "step checkpoints (use ILC_ADJOINT_RECOMPUTE to avoid them)");
+    ILC_CUDA(c, c.rec_n.ensure((size_t)npix * 4), "step counts");
+    ra.rec_h = c.rec_h.as<float>();
+    ra.rec_n = c.rec_n.as<int32_t>();
+  }
+  float fwd_ms = 0.0f;
+  ILC_CUDA(c, render_launch(c, ra, &fwd_ms), "forward render");
+  uint32_t flags = 0;
+  DevStats fs{};
+  st = read_flags(c, &flags, &fs);
+  if (st) return st;
+  if (flags & FLAG_STEP_LIMIT) return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the step limit");
+  if (flags & FLAG_REC_OVERFLOW) return fail(c, ILC_ERR_INTERNAL, "step checkpoint overflow");
+  // 4. loss and per-pixel seed
+  const void* dtarget = nullptr;
+  ILC_CUDA(c, stage_in(c, c.in_a, target, (size_t)npix * 4, is_device, &dtarget), "target");
+  ILC_CUDA(c, c.adj_seed.ensure((size_t)npix * 4), "seed");
+  ILC_CUDA(c, c.adj_loss.ensure(8), "loss");
+  ILC_CUDA(c, adjoint_seed_launch(c, ra.out, static_cast<const float*>(dtarget), npix, ra.scale,
+                                  c.adj_seed.as<float>(), c.adj_loss.as<double>()),
+           "loss kernel");
+  // 5. adjoint rays
+  ILC_CUDA(c, c.adj_grad.ensure(n * 4), "gradient");
+  ILC_CUDA(c, cudaMemsetAsync(c.adj_grad.p, 0, n * 4, c.stream), "gradient");
+  float adj_ms = 0.0f;
+  ILC_CUDA(c, adjoint_ray_launch(c, ra, mode, c.adj_seed.as<float>(), c.adj_grad.as<float>(),
+                                 &adj_ms),
+           "adjoint kernel");
+  DevStats as{};
+  st = read_flags(c, &flags, &as);
+  if (st) return st;
+  if (flags & FLAG_STEP_LIMIT) return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the step limit");
+  // 6. chain rule into the caller's arrays
+  void *gr = nullptr, *gt = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, dL_dlnrho, n * 4, is_device, &gr), "dL/dlnrho");
+  ILC_CUDA(c, out_ptr(c.out_c, dL_dlnT, n * 4, is_device, &gt), "dL/dlnT");
+  ILC_CUDA(c, adjoint_chain_launch(c, c.adj_grad.as<float>(), n, c.adj_dR.as<float>(),
+                                   c.adj_dT.as<float>(), static_cast<float*>(gr),
+                                   static_cast<float*>(gt)),
+           "chain rule kernel");
+  const cudaMemcpyKind k = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  ILC_CUDA(c, cudaMemcpyAsync(image, ra.out, (size_t)npix * 4, k, c.stream), "image out");
+  if (!is_device) {
+    ILC_CUDA(c, cudaMemcpyAsync(dL_dlnrho, gr, n * 4, cudaMemcpyDeviceToHost, c.stream), "D2H");
+    ILC_CUDA(c, cudaMemcpyAsync(dL_dlnT, gt, n * 4, cudaMemcpyDeviceToHost, c.stream), "D2H");
+  }
+  double loss = 0.0;
+  ILC_CUDA(c, cudaMemcpyAsync(&loss, c.adj_loss.p, 8, cudaMemcpyDeviceToHost, c.stream), "loss");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "adjoint");
+  float qms = 0.0f;
+  cudaEventElapsedTime(&qms, q0, q1);
+  cudaEventDestroy(q0);
+  cudaEventDestroy(q1);
+  if (stats) {
+    stats->loss = loss;
+    stats->quantity_ms = qms;
+    stats->forward_ms = fwd_ms;
+    stats->adjoint_ms = adj_ms;
+    stats->forward_steps = fs.steps;
+    stats->adjoint_steps = as.steps;
+  }
+  return ILC_OK;
+}
 
 ilc_status ilc_autotune_z_window(ilc_ctx* h, const ilc_camera* cam, double z_range,
                                  ilc_tolerance tol, int32_t controller, const float* candidates,

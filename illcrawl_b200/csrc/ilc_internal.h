@@ -77,6 +77,9 @@ struct Context {
   DevBuf flags;      // uint32 error flags + uint64 stats
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   uint64_t launches = 0;  // kernels this context has launched
+
+  // adjoint: step checkpoints, per-cell derivatives, gradient accumulator
+  DevBuf rec_h, rec_n, adj_dT, adj_dR, adj_grad, adj_seed, adj_loss;
 };
 
 // Error flags written by kernels (bit mask in flags[0]).
@@ -84,6 +87,7 @@ enum : uint32_t {
   FLAG_KEY_RANGE = 1u,
   FLAG_STEP_LIMIT = 2u,
   FLAG_NONFINITE = 4u,
+  FLAG_REC_OVERFLOW = 8u,
 };
 
 // Stats block layout behind the flags word (uint64 counters).
@@ -128,7 +132,26 @@ struct RenderArgs {
   float* out;           // device image
   float window_override = -1.0f;  // >= 0: z window for this launch (autotuner)
   int row_stride = 1;             // > 1: only every row_stride-th tile row (autotuner)
+  float* rec_h = nullptr;         // adjoint checkpoint: accepted step sizes per ray
+  int32_t* rec_n = nullptr;
+  int64_t rec_cap = 0;
 };
+
+// Adjoint of the X-ray band map (ilc_adjoint.cu).
+// q (stride q_stride floats), dq/dlnT and dq/dlnrho per cell, original order.
+cudaError_t adjoint_cell_launch(Context& c, const float* rho, const float* u, const float* xe,
+                                uint64_t n, float z, float dL, float emin, float emax,
+                                int num_samples, float* q_out, int q_stride, float* dq_lnT,
+                                float* dq_lnrho);
+// loss (double, accumulated) and dL/dI_raw seed per pixel
+cudaError_t adjoint_seed_launch(Context& c, const float* img, const float* target, int64_t npix,
+                                float scale, float* seed, double* loss);
+// replay (checkpoint) or recompute the rays and scatter dL/dq (sorted order)
+cudaError_t adjoint_ray_launch(Context& c, const RenderArgs& a, int mode, const float* seed,
+                               float* grad, float* kernel_ms);
+// dL/dln rho, dL/dln T in the original order
+cudaError_t adjoint_chain_launch(Context& c, const float* grad, uint64_t n, const float* dq_lnrho,
+                                 const float* dq_lnT, float* g_lnrho, float* g_lnT);
 cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms);
 
 // Spiral table (8 subcells x 125 offsets), generated on the host.

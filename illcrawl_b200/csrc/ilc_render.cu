@@ -38,6 +38,9 @@ struct RenderK {
   int64_t max_steps;
   float window;     // z window of the adaptive schedule (<= 0: none)
   int row_stride;   // render every row_stride-th row of tiles (1 = all)
+  float* rec_h;     // optional: accepted step sizes per ray (ray-major, rec_cap each)
+  int32_t* rec_n;   // optional: number of accepted steps per ray
+  int64_t rec_cap;
   float scale;
   int apply_scale;
   float* out;
@@ -100,15 +103,23 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
         if ((int64_t)steps >= a.max_steps) { at_limit = true; run = false; break; }
         float e[4];
         nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
-        const float zb = z;
+        const float zb = z, hb = h;
         if (a.controller == ILC_CONTROLLER_REF32)
           rkf_advance_ref32(I, z, h, k1, fa, fr, a.z_end, e, kEps, kHmin, kHmax, pts);
         else
           rkf_advance_fp64(I, z, h, k1, a.atol, a.rtol, a.z_end, e, kEps, kHmin, kHmax, pts);
         ++steps;
-        if (z != zb) ++acc;
+        if (z != zb) {
+          if (a.rec_h && (int64_t)acc < a.rec_cap)
+            a.rec_h[((int64_t)iy * a.cam.nx + ix) * a.rec_cap + (int64_t)acc] = hb;
+          ++acc;
+        }
       }
       wend = a.window > 0.0f ? wend + a.window : a.z_end;
+    }
+    if (active && a.rec_n) {
+      a.rec_n[(int64_t)iy * a.cam.nx + ix] = (int32_t)min((int64_t)acc, a.rec_cap);
+      if ((int64_t)acc > a.rec_cap) atomicOr(flags, FLAG_REC_OVERFLOW);
     }
   }
   if (active) a.out[(size_t)iy * a.cam.nx + ix] = a.apply_scale ? I * a.scale : I;
@@ -157,6 +168,9 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   k.max_steps = c.max_steps;
   k.window = a.window_override >= 0.0f ? a.window_override : c.z_window;
   k.row_stride = a.row_stride > 1 ? a.row_stride : 1;
+  k.rec_h = a.rec_h;
+  k.rec_n = a.rec_n;
+  k.rec_cap = a.rec_cap;
   k.scale = a.scale;
   k.apply_scale = a.apply_scale ? 1 : 0;
   k.out = a.out;

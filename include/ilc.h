@@ -213,6 +213,37 @@ ilc_status ilc_project_xray_flux(ilc_ctx* ctx, const float* cells, const float* 
                                  const ilc_los_scaling* scaling, float* image, int is_device,
                                  ilc_render_stats* stats);
 
+/* ---- adjoint ------------------------------------------------------------
+ * Gradient of L = sum over pixels of (log I - log I_target)^2 for the X-ray
+ * band map of ilc_project_xray_flux, with respect to per-cell ln rho and
+ * ln T, the neighbour choice fixed and the line-of-sight step sequence frozen
+ * from the forward pass. No reference counterpart (the reference has no
+ * differentiation). CHECKPOINT stores every ray's accepted step sizes during
+ * the forward pass (4 B x (z_range / 0.2 + 2) per ray of device memory) and
+ * replays them; RECOMPUTE runs the step controller again instead. Pixels whose
+ * value or target is not positive are left out of L. The per-cell factors
+ * dq/dln rho and dq/dln T are exact derivatives of the adaptive energy
+ * integration of xray_flux. image receives the forward band map. */
+enum { ILC_ADJOINT_CHECKPOINT = 0, ILC_ADJOINT_RECOMPUTE = 1 };
+
+typedef struct ilc_adjoint_stats {
+  double loss;
+  float quantity_ms;   /* per-cell flux + derivatives */
+  float forward_ms;    /* forward render kernel (with step recording in CHECKPOINT) */
+  float adjoint_ms;    /* adjoint render kernel */
+  uint64_t forward_steps;
+  uint64_t adjoint_steps;
+} ilc_adjoint_stats;
+
+ilc_status ilc_adjoint_xray_flux(ilc_ctx* ctx, const float* cells, const float* rho,
+                                 const float* u, const float* xe, uint64_t n, float redshift,
+                                 float luminosity_distance, float e_min, float e_max,
+                                 int32_t num_samples, const ilc_camera* cam, double z_range,
+                                 ilc_tolerance tol, int32_t controller,
+                                 const ilc_los_scaling* scaling, const float* target, int32_t mode,
+                                 float* image, float* dL_dlnrho, float* dL_dlnT, int is_device,
+                                 ilc_adjoint_stats* stats);
+
 /* Autotuner of the adaptive render's schedule: renders every sample_stride-th
  * row of 8-pixel tiles of the view once per candidate z window, times the
  * render kernel with CUDA events, sets the fastest on the context and returns

@@ -1,0 +1,65 @@
+"""GPU adjoint through the C ABI against the FP64 oracle adjoint on the same
+frozen step sequences (the oracle adjoint itself is pinned by central finite
+differences in test_adjoint_oracle.py)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+Z, DL, EMIN, EMAX, NS = 0.2, 978500.0, 0.5, 7.0, 100
+
+
+def _setup(oracle_mod, gaunt_table, n=20_000, nx=24, seed=41):
+    import illcrawl_b200 as ilc
+    from illcrawl_b200 import synthetic
+    c = synthetic.small_cells(n, seed=seed, box=400.0, r_s=50.0)
+    args = ((200, 200, 0), (0, 0, 1), 0.0, 160.0, nx, nx)
+    q, dqT, dqR = oracle_mod.xray_band_grad(gaunt_table, c.rho, c.u, c.xe, Z, DL, EMIN, EMAX,
+                                            NS, precision=0)
+    g = oracle_mod.Grid(c.xyzq(q))
+    I, hs, nacc, rc = g.render_record(oracle_mod.camera(*args), 400.0, 0.0, 1e-3, mode=1,
+                                      cap=4096)
+    assert rc == 0
+    rng = np.random.default_rng(seed)
+    target = (I * np.exp(0.3 * rng.normal(size=I.shape))).astype(np.float32)
+    return ilc, c, args, q, dqT, dqR, g, I, hs, nacc, target
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_gpu_adjoint_matches_fp64_oracle(ctx, oracle_mod, gaunt_table, mode):
+    ilc, c, args, q, dqT, dqR, g, I, hs, nacc, target = _setup(oracle_mod, gaunt_table)
+    ctx.load_gaunt()
+    cells = c.xyzq(np.zeros(c.n, np.float32))
+    img, gr, gt, st = ctx.adjoint_xray_flux(cells, c.rho, c.u, c.xe, ilc.camera(*args), 400.0,
+                                            target.reshape(args[5], args[4]), mode=mode,
+                                            e_min=EMIN, e_max=EMAX)
+    # forward image: bit-exact with the oracle's (FP64 controller)
+    assert np.array_equal(img.ravel().view(np.uint32), I.view(np.uint32))
+    Id = I.astype(np.float64)
+    loss = np.sum((np.log(Id) - np.log(target.astype(np.float64))) ** 2)
+    assert st["loss"] == pytest.approx(loss, rel=1e-9)
+    gI = 2.0 * (np.log(Id) - np.log(target.astype(np.float64))) / Id
+    grad_q = oracle_mod.adjoint(g, oracle_mod.camera(*args), hs, nacc, gI, precision=1)
+    want_r, want_t = grad_q * dqR, grad_q * dqT
+    for got, want in ((gr, want_r), (gt, want_t)):
+        got = got.astype(np.float64)
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert err < 1e-3, err
+        big = np.abs(want) > 1e-2 * np.abs(want).max()
+        assert np.max(np.abs(got[big] - want[big]) / np.abs(want[big])) < 1e-3
+    assert st["forward_ms"] > 0 and st["adjoint_ms"] > 0
+
+
+def test_gpu_adjoint_checkpoint_equals_recompute(ctx, oracle_mod, gaunt_table):
+    ilc, c, args, q, dqT, dqR, g, I, hs, nacc, target = _setup(oracle_mod, gaunt_table, seed=42)
+    ctx.load_gaunt()
+    cells = c.xyzq(np.zeros(c.n, np.float32))
+    t = target.reshape(args[5], args[4])
+    _, r0, t0, s0 = ctx.adjoint_xray_flux(cells, c.rho, c.u, c.xe, ilc.camera(*args), 400.0, t,
+                                          mode=0)
+    _, r1, t1, s1 = ctx.adjoint_xray_flux(cells, c.rho, c.u, c.xe, ilc.camera(*args), 400.0, t,
+                                          mode=1)
+    # same terms, summed by float atomics in a different order
+    assert np.linalg.norm(r0 - r1) / np.linalg.norm(r0) < 1e-5
+    assert np.linalg.norm(t0 - t1) / np.linalg.norm(t0) < 1e-5
+    assert s0["loss"] == s1["loss"]
