@@ -98,6 +98,7 @@ SIGNATURES = {
     "ilc_project_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
                                      _f64, Tolerance, _i32, _P, _P, _int, _P]),
     "ilc_kernel_launches": (_u64, [_P]),
+    "ilc_grid_build_noalloc": (_int, [_P, _u64, _P, _P, _u64, _P, _P, _P]),
     "ilc_autotune_z_window": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _i32, _i32, _P, _P]),
     "ilc_adjoint_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
                                      _f64, Tolerance, _i32, _P, _P, _i32, _P, _P, _P, _int, _P]),

@@ -317,3 +317,139 @@ void spiral_table(int8_t out[8][125][3]) {
 }
 
 }  // namespace ilc
+
+// ---------------------------------------------------------------------------
+// Allocation-free grid build.
+//
+// Some callers cannot allocate device memory at the point where they need a
+// grid: code running while a CUDA graph is being captured (cudaMalloc is not a
+// capturable operation), real-time loops with a fixed memory budget, or hosts
+// whose allocator owns every device buffer. ilc_grid_build_noalloc builds the
+// same particle grid as ilc_nn8_setup_particles without any allocation: the
+// caller passes device buffers for the inputs and outputs, and the sort's
+// scratch space is this file-scope device array, sized for at most
+// ILC_NOALLOC_MAX_PARTICLES particles (about 16.5 MiB, held on every GPU that
+// loads the library until the process exits).
+// ---------------------------------------------------------------------------
+namespace ilc {
+namespace {
+
+constexpr uint64_t kNoAllocMax = 1ull << 20;  // ILC_NOALLOC_MAX_PARTICLES
+constexpr uint64_t kNoAllocTiles = (kNoAllocMax + 2047) / 2048;
+// [0, 64): bounding-box words; [64, 128): flags; then keys a/b, values a/b,
+// and the radix histogram.
+constexpr size_t kOffKeysA = 256;
+constexpr size_t kOffKeysB = kOffKeysA + 4 * kNoAllocMax;
+constexpr size_t kOffValsA = kOffKeysB + 4 * kNoAllocMax;
+constexpr size_t kOffValsB = kOffValsA + 4 * kNoAllocMax;
+constexpr size_t kOffHist = kOffValsB + 4 * kNoAllocMax;
+constexpr size_t kScratchBytes = kOffHist + 4 * 256 * kNoAllocTiles;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current (in host code the symbol is only a host-side
+// stand-in for the array, not a device address).
+constexpr int kMaxDevices = 64;
+static void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+}  // namespace
+}  // namespace ilc
+
+extern "C" ilc_status ilc_grid_build_noalloc(const float* particles, uint64_t n,
+                                             float* sorted_particles, int32_t* cells,
+                                             uint64_t cells_capacity,
+                                             uint32_t* sorted_to_unsorted, ilc_grid_desc* desc,
+                                             void* stream) {
+  using namespace ilc;
+  if (!particles || !sorted_particles || !cells || !sorted_to_unsorted || !desc || n == 0)
+    return ILC_ERR_INVALID_ARGUMENT;
+  if (n > kNoAllocMax) return ILC_ERR_INVALID_ARGUMENT;  // beyond the scratch array
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ILC_ERR_CUDA;
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ILC_ERR_CUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  unsigned char* s = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float4* in = reinterpret_cast<const float4*>(particles);
+  unsigned* acc = reinterpret_cast<unsigned*>(s);
+  uint32_t* flags = reinterpret_cast<uint32_t*>(s + 64);
+  // bounding box (the words must start at +/- extremes, the flags at zero)
+  const unsigned init[8] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u, 0u, 0u};
+  if (cudaMemcpyAsync(acc, init, sizeof(init), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemsetAsync(flags, 0, 64, st) != cudaSuccess)
+    return ILC_ERR_CUDA;
+  bbox_kernel<<<(unsigned)std::min<uint64_t>(grid_blocks(n, 256), 148 * 8), 256, 0, st>>>(in, n,
+                                                                                         acc);
+  unsigned box[8];
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(box, acc, sizeof(box), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return ILC_ERR_CUDA;
+  if (box[6]) return ILC_ERR_NONFINITE_INPUT;
+  // grid parameters in double, as particle_grid.cpp:54-103
+  double mn[3], mx[3], vol = 1.0;
+  for (int k = 0; k < 3; ++k) {
+    unsigned b;
+    float f;
+    ord2f_bits(box[k], &b);
+    std::memcpy(&f, &b, 4);
+    mn[k] = (double)f - 0.1;
+    ord2f_bits(box[3 + k], &b);
+    std::memcpy(&f, &b, 4);
+    mx[k] = (double)f + 0.1;
+    vol *= (mx[k] - mn[k]);
+  }
+  const double w = std::cbrt((double)8 / (double)n * vol);
+  KeyGrid kg;
+  int32_t nc[3];
+  uint64_t total = 1;
+  for (int k = 0; k < 3; ++k) {
+    nc[k] = (int32_t)std::ceil((mx[k] - mn[k]) / w);
+    desc->min_corner[k] = (float)mn[k];
+    desc->cell_sizes[k] = (float)w;
+    desc->num_cells[k] = nc[k];
+    total *= (uint64_t)(nc[k] > 0 ? nc[k] : 0);
+  }
+  desc->total_cells = total;
+  desc->num_particles = n;
+  if (total == 0 || total >= (1ull << 32)) return ILC_ERR_GRID_TOO_LARGE;
+  if (total > cells_capacity) return ILC_ERR_INVALID_ARGUMENT;  // desc says how many are needed
+  kg.min0 = desc->min_corner[0]; kg.min1 = desc->min_corner[1]; kg.min2 = desc->min_corner[2];
+  kg.cs0 = desc->cell_sizes[0]; kg.cs1 = desc->cell_sizes[1]; kg.cs2 = desc->cell_sizes[2];
+  kg.n0 = nc[0]; kg.n1 = nc[1];
+  kg.total = total;
+  uint32_t* ka = reinterpret_cast<uint32_t*>(s + kOffKeysA);
+  uint32_t* kb = reinterpret_cast<uint32_t*>(s + kOffKeysB);
+  uint32_t* va = reinterpret_cast<uint32_t*>(s + kOffValsA);
+  uint32_t* vb = reinterpret_cast<uint32_t*>(s + kOffValsB);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(s + kOffHist);
+  keys_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(in, n, kg, ka, va, flags);
+  const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+  int bits = 1;
+  while (bits < 32 && (1ull << bits) < total) ++bits;
+  for (int shift = 0; shift < bits; shift += 8) {
+    radix_hist_kernel<<<(unsigned)tiles, kSortThreads, 0, st>>>(ka, n, shift, (uint32_t)tiles,
+                                                                 hist);
+    scan_kernel<<<1, 1024, 0, st>>>(hist, tiles * 256);
+    radix_scatter_kernel<<<(unsigned)tiles, kSortThreads, 0, st>>>(ka, va, n, shift,
+                                                                   (uint32_t)tiles, hist, kb, vb);
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  gather_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(in, va, n,
+                                                      reinterpret_cast<float4*>(sorted_particles),
+                                                      sorted_to_unsorted);
+  if (cudaMemsetAsync(cells, 0, total * 8, st) != cudaSuccess) return ILC_ERR_CUDA;
+  cell_ranges_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(ka, n, reinterpret_cast<int2*>(cells));
+  uint32_t f = 0;
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(&f, flags, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return ILC_ERR_CUDA;
+  if (f & FLAG_KEY_RANGE) return ILC_ERR_INTERNAL;
+  return ILC_OK;
+}

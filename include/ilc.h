@@ -255,6 +255,30 @@ ilc_status ilc_autotune_z_window(ilc_ctx* ctx, const ilc_camera* cam, double z_r
                                  int32_t n_candidates, int32_t sample_stride, float* best,
                                  float* times_ms);
 
+/* Allocation-free grid build, for callers that cannot allocate device memory
+ * when they need a grid (for example while a CUDA graph is being captured, in
+ * a real-time loop with a fixed memory budget, or under a host allocator that
+ * owns all device buffers). No counterpart in the reference. It builds the
+ * same grid as ilc_nn8_setup_particles into caller-owned device buffers:
+ * particles (n float4), sorted_particles (n float4), cells (cells_capacity
+ * int2), sorted_to_unsorted (n uint32), all on the current device; desc
+ * receives the grid parameters (also when cells_capacity is too small, so the
+ * caller can size the cells buffer and call again). It allocates nothing: the
+ * sort's scratch is a fixed device array inside the library, sized for at
+ * most ILC_NOALLOC_MAX_PARTICLES particles (about 16.5 MiB per GPU that loads
+ * the library, held until the process exits); larger n is rejected with
+ * ILC_ERR_INVALID_ARGUMENT. The first call on a device looks the array's
+ * device address up once, so make that first call before any stream capture.
+ * Every call shares the one scratch array: calls whose work overlaps on the
+ * GPU (different streams or host threads at the same time) race. Work is
+ * issued on `stream` (a cudaStream_t, NULL = default stream) and has finished
+ * when the call returns. */
+#define ILC_NOALLOC_MAX_PARTICLES 1048576
+ilc_status ilc_grid_build_noalloc(const float* particles, uint64_t n, float* sorted_particles,
+                                  int32_t* cells, uint64_t cells_capacity,
+                                  uint32_t* sorted_to_unsorted, ilc_grid_desc* desc,
+                                  void* stream);
+
 /* Number of kernels this context has launched so far. */
 uint64_t ilc_kernel_launches(const ilc_ctx* ctx);
 
