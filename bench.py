@@ -99,26 +99,77 @@ TUNING_FILE = os.path.join(ROOT, "illcrawl_b200", "data", "render_tuning.json")
 
 
 def tune_schedule(ctx, cam, args, gpu_name):
-    """z window of the adaptive render: --z-window if given, else the cached
-    autotuner result for this workload and GPU, else run the autotuner (a
-    sample of tile rows per candidate, outside the timed region) and cache."""
+    """Schedule of the render kernel (orders work only, never changes a
+    result). Persistent engine: tile shape, blocks per SM and z window from
+    the cache for this GPU and workload, else defaults; --autotune re-runs the
+    autotuner on the same camera at half resolution (8,192 tiles) and caches
+    the winner. Grid engine: z window and occupancy, likewise."""
     import illcrawl_b200 as ilc
-    if args.z_window is not None:
-        ctx.set_z_window(args.z_window)
-        return {"z_window": args.z_window, "source": "command line"}
-    key = f"{gpu_name}|xray_band_map_4M_cells_{NX}sq_rtol1e-3|z0={Z_START}|depth={DEPTH}"
     cache = json.load(open(TUNING_FILE)) if os.path.exists(TUNING_FILE) else {}
-    if key in cache:
-        ctx.set_z_window(cache[key]["z_window"])
-        return dict(cache[key], source="cache")
-    best, times = ctx.autotune_z_window(cam, DEPTH, REL_TOL, 0.0, ilc.CONTROLLER_FP64,
-                                        sample_stride=max(1, NY // 64))
-    cache[key] = {"z_window": best, "kernel_ms": times}
+    base = f"{gpu_name}|xray_band_map_4M_cells_{NX}sq_rtol1e-3|z0={Z_START}|depth={DEPTH}"
+    if args.engine == "grid":
+        ctx.set_render_engine(ilc.ENGINE_GRID)
+        if args.z_window is not None:
+            ctx.set_z_window(args.z_window)
+            return {"engine": "grid", "z_window": args.z_window, "source": "command line"}
+        key = base
+        if key in cache and not args.autotune:
+            ctx.set_z_window(cache[key]["z_window"])
+            ctx.set_render_occupancy(cache[key]["occupancy"])
+            return dict(cache[key], engine="grid", source="cache")
+        bw, bo, times = ctx.autotune_render(cam, DEPTH, REL_TOL, 0.0, ilc.CONTROLLER_FP64,
+                                            sample_stride=max(1, NY // 64))
+        cache[key] = {"z_window": bw, "occupancy": bo,
+                      "kernel_ms": {f"w{w}_o{o}": t for (w, o), t in times.items()}}
+        src = "autotuner"
+    else:
+        ctx.set_render_engine(ilc.ENGINE_PERSISTENT)
+        key = base + "|persistent"
+        if args.z_window is not None:
+            ctx.set_batch_schedule(8, 3, args.z_window, True)
+            return {"engine": "persistent", "tile_w": 8, "occupancy": 3,
+                    "z_window": args.z_window, "source": "command line"}
+        if key in cache and not args.autotune:
+            e = cache[key]
+            ctx.set_batch_schedule(e["tile_w"], e["occupancy"], e["z_window"], True)
+            return dict(e, engine="persistent", source="cache")
+        if not args.autotune:
+            ctx.set_batch_schedule(8, 3, 40.0, True)
+            return {"engine": "persistent", "tile_w": 8, "occupancy": 3, "z_window": 40.0,
+                    "source": "default"}
+        half = ilc.camera(*camera_args()[:4], NX // 2, NY // 2)
+        q = ctx.tuning_values
+        bt, bo, bw, times = ctx.autotune_batched(q, [ilc.job(half, z_range=DEPTH)], REL_TOL, 0.0,
+                                                 tile_ws=(4, 8, 16, 32), occupancies=(0, 3),
+                                                 windows=(0.0, 20.0, 80.0))
+        cache[key] = {"tile_w": bt, "occupancy": bo, "z_window": bw,
+                      "kernel_ms": {f"t{t}_o{o}_w{w}": v for (t, o, w), v in times.items()}}
+        src = "autotuner"
     try:
         json.dump(cache, open(TUNING_FILE, "w"), indent=1, sort_keys=True)
     except OSError:
         pass
-    return dict(cache[key], source="autotuner")
+    return dict(cache[key], engine=args.engine, source=src)
+
+
+def max_over_ranks(value, device):
+    """The slowest rank's time (every rank takes this collective in the same
+    order). Replicas share nothing else: no data-path collective."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank, seconds_per_rank, device):
+    """Whole-job throughput of N replicas: all ranks' units / the slowest
+    rank's time."""
+    import torch.distributed as dist
+    world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+    return units_per_rank * world / max_over_ranks(seconds_per_rank, device)
 
 
 def make_inputs():
@@ -157,6 +208,103 @@ def cpu_baseline(cells, nthreads, sample_rays=2048, seed=1):
     t_render = time.perf_counter() - t0
     t_full = t_fixed + t_render * (NX * NY) / sample_rays
     return NX * NY / t_full / 1e6, t_fixed, t_render
+
+
+def spectrum_jobs(ilc, div, seed=20172):
+    """The batched uneven workload: 48 seeded cameras around the halo, sides
+    drawn from {256, 512, 768, 1024} (divided by div for a bounded sample),
+    circular apertures of radius U(0.5, 3) Mpc, every ray over its chord of
+    the r = 3 Mpc sphere, widened to at least 0.6 Mpc (a 10x spread)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    centre = np.full(3, BOX / 2)
+    jobs = []
+    for _ in range(48):
+        v = rng.normal(size=3)
+        look = v / np.linalg.norm(v)
+        side = int(rng.choice([256, 512, 768, 1024])) // div
+        cam = ilc.camera(tuple(centre - 3500.0 * look), tuple(look),
+                         float(rng.uniform(0.0, 2.0 * np.pi)), BOX, side, side)
+        jobs.append(ilc.job(cam, aperture_radius=float(rng.uniform(500.0, 3000.0)),
+                            sphere_center=tuple(centre), sphere_radius=3000.0,
+                            min_chord=600.0))
+    return jobs
+
+
+def batched_leg(ctx, ilc, torch, d_rho, d_u, d_xe, args):
+    """Batched vs plain on the uneven spectral workload: 128 log-spaced bins
+    over 0.3-10 keV. Batched: one persistent launch for all cameras and bins.
+    Plain: one launch per (camera, bin) image, as the reference renders a
+    spectrum; timed on args.plain_bins bins spread over the band and scaled to
+    128 (each bin's render has the same structure)."""
+    edges = np.geomspace(0.3, 10.0, 129)
+    e = edges[:-1].astype(np.float32)
+    w = np.diff(edges).astype(np.float32)
+    tab = ctx.xray_spectrum(d_rho, d_u, d_xe, e, w)
+    jobs = spectrum_jobs(ilc, args.batched_div)
+    ctx.render_batched(tab, jobs)            # warm-up (also the cost-order pass)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, st = ctx.render_batched(tab, jobs)
+    torch.cuda.synchronize()
+    t_batched = time.perf_counter() - t0
+    bins = np.linspace(0, 127, args.plain_bins).round().astype(int)
+    t_plain = 0.0
+    k_plain = 0.0
+    rays = 0
+    for b in bins:
+        vb = tab[:, int(b)].contiguous()
+        for j in jobs:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, sj = ctx.render_batched(vb, [j])
+            torch.cuda.synchronize()
+            t_plain += time.perf_counter() - t0
+            k_plain += sj["kernel_ms"] * 1e-3
+    masked = 0
+    for j in jobs:
+        n = j.camera.num_pix_x
+        ps = BOX / n
+        c = (np.arange(n) + 0.5 - 0.5 * n) * ps
+        masked += int(np.sum(c[:, None] ** 2 + c[None, :] ** 2 <= j.aperture_radius ** 2))
+    rays = masked
+    plain_128 = t_plain / len(bins) * 128
+    return {"workload": f"48 cameras, sides {{256..1024}}/{args.batched_div}, apertures 0.5-3 Mpc, "
+                        "chords of the 3 Mpc sphere, 128 bins 0.3-10 keV, rtol 1e-3",
+            "rays": rays, "bins": 128,
+            "batched_s": t_batched, "batched_kernel_s": st["kernel_ms"] * 1e-3,
+            "batched_mrays_per_s": rays / t_batched / 1e6,
+            "plain_s_128_bins": plain_128, "plain_bins_timed": int(len(bins)),
+            "plain_kernel_s_128_bins": k_plain / len(bins) * 128,
+            "plain_mrays_per_s": rays / plain_128 / 1e6,
+            "batched_over_plain": plain_128 / t_batched, "batched_stats": st}
+
+
+def adjoint_leg(ctx, ilc, cells, args):
+    """Adjoint cost on the 512^2 band map: loss sum (log I - log I_t)^2 with
+    I_t rendered from the same cells with log T + a seeded Gaussian random
+    field (sigma 0.1, correlation length 200 kpc); gradient with respect to
+    per-cell log rho and log T. adjoint/forward = adjoint kernel time over the
+    forward render time of the same call."""
+    from illcrawl_b200 import synthetic
+    side = 512
+    cam = ilc.camera((BOX / 2, BOX / 2, Z_START), (0.0, 0.0, 1.0), 0.0, BOX, side, side)
+    field = synthetic.gaussian_random_field_at(cells.pos, BOX, 0.1, 200.0, 256, 20174)
+    u_t = synthetic.perturbed_internal_energy(cells, field)
+    xyz4 = cells.xyzq(np.zeros(cells.n, np.float32))
+    target, _ = ctx.project_xray_flux(xyz4, cells.rho, u_t, cells.xe, cam, DEPTH,
+                                      rel_tol=REL_TOL, e_min=E_MIN, e_max=E_MAX,
+                                      num_samples=NUM_SAMPLES)
+    out = {"workload": "512^2 band map, 4,194,304 cells, target log T + GRF(0.1, 200 kpc)"}
+    for name, mode in (("checkpoint", ilc._lib.ADJOINT_CHECKPOINT),
+                       ("recompute", ilc._lib.ADJOINT_RECOMPUTE)):
+        _, _, _, st = ctx.adjoint_xray_flux(xyz4, cells.rho, cells.u, cells.xe, cam, DEPTH,
+                                            target, mode=mode, rel_tol=REL_TOL,
+                                            e_min=E_MIN, e_max=E_MAX, num_samples=NUM_SAMPLES)
+        out[name] = {"forward_ms": st["forward_ms"], "adjoint_ms": st["adjoint_ms"],
+                     "quantity_ms": st["quantity_ms"],
+                     "adjoint_over_forward": st["adjoint_ms"] / st["forward_ms"],
+                     "loss": st["loss"]}
+    return out
 
 
 def run_reference(args, rank, world):
@@ -203,8 +351,6 @@ def run_ours(args, rank, world, local_rank):
     n = cells.n
     ctx = ilc.Context(local_rank)
     ctx.load_gaunt()
-    if args.z_window is not None:
-        ctx.set_z_window(args.z_window)
     cam = ilc.camera(*camera_args())
     scaling = ilc.LosScaling(1.0, 1.0, ilc.DA_PIXEL_AREA)
     dev = torch.device("cuda", local_rank)
@@ -219,11 +365,17 @@ def run_ours(args, rank, world, local_rank):
                                      controller=ilc.CONTROLLER_FP64, e_min=E_MIN, e_max=E_MAX,
                                      num_samples=NUM_SAMPLES, scaling=scaling, image=d_img)
 
+    tuned = None
+    ctx.set_render_engine(ilc.ENGINE_PERSISTENT if args.engine == "persistent"
+                          else ilc.ENGINE_GRID)
     for i in range(max(args.warmup, 1)):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         step()
-        if i == 0:
+        if i == 0:  # the schedule only orders work: tuned after the first step
+            if args.autotune and args.engine == "persistent":
+                ctx.tuning_values = ctx.xray_flux(d_rho, d_u, d_xe, REDSHIFT, DL, E_MIN, E_MAX,
+                                                  NUM_SAMPLES)
             tuned = tune_schedule(ctx, cam, args, torch.cuda.get_device_name(dev))
     if dist:
         dist.barrier()
@@ -245,12 +397,10 @@ def run_ours(args, rank, world, local_rank):
     launches = ctx.kernel_launches - launches0
     if dist:
         dist.barrier()
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dev)
     ms_per_step = total_ms / args.steps
     rays = NX * NY * world
-    value = rays / (ms_per_step * 1e-3) / 1e6
+    value = replica_value(NX * NY, ms_per_step * 1e-3, dev) / 1e6
 
     # e2e: host (pinned) buffers through the public API
     h_cells = torch.from_numpy(xyz4).pin_memory()
@@ -279,12 +429,13 @@ def run_ours(args, rank, world, local_rank):
             e2e_step()
             e2e_s += time.perf_counter() - t0
         e2e_s /= e2e_steps
-        if dist:
-            t = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e_value = rays / e2e_s / 1e6
+        e2e_value = replica_value(NX * NY, e2e_s, dev) / 1e6
 
+    extra = {}
+    if world == 1 and not args.no_batched:
+        extra["batched"] = batched_leg(ctx, ilc, torch, d_rho, d_u, d_xe, args)
+    if world == 1 and not args.no_adjoint:
+        extra["adjoint"] = adjoint_leg(ctx, ilc, cells, args)
     if rank != 0:
         ctx.close()
         return
@@ -306,7 +457,8 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(4 * NX * NY)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None,
-                     "peak_kind": peak_kind, "kernel": "render_kernel",
+                     "peak_kind": peak_kind,
+                     "kernel": "batched_kernel" if args.engine == "persistent" else "render_kernel",
                      "kernel_ms": last_stats["kernel_ms"], "algorithmic_bytes": kbytes},
         "cpu_baseline": {"value": cpu_v, "unit": "Mrays/s", "cores": cores, "kind": "port",
                          "sample": "per-cell X-ray flux + grid build over all 4,194,304 cells "
@@ -315,6 +467,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches,
         "render_stats": last_stats,
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -331,6 +484,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
     ap.add_argument("--z-window", type=float, default=None,
                     help="z window of the adaptive schedule in kpc (default: the tuned value)")
+    ap.add_argument("--engine", default="persistent", choices=["persistent", "grid"],
+                    help="render kernel: persistent work queue (default) or one block per tile")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-vs-plain spectral leg")
+    ap.add_argument("--batched-div", type=int, default=4,
+                    help="camera sides of the batched leg divided by this (bounded sample)")
+    ap.add_argument("--plain-bins", type=int, default=4,
+                    help="bins timed in the plain per-(camera, bin) arm, scaled to 128")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
+    ap.add_argument("--autotune", action="store_true",
+                    help="re-run the schedule autotuner and update the cache")
     ap.add_argument("--z-start", type=float, default=0.0,
                     help="camera plane position along z (profiling cases only)")
     ap.add_argument("--z-range", type=float, default=None,

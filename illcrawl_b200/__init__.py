@@ -21,7 +21,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (CONTROLLER_FP64, CONTROLLER_REF32, DA_INVERSE_RANGE, DA_PIXEL_AREA, DA_UNIT,
-                   Camera, IlcError, LosScaling, RenderStats, Tolerance)
+                   ENGINE_GRID, ENGINE_PERSISTENT, Camera, IlcError, Job, LosScaling, RenderStats, Tolerance)
 
 DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 GAUNT_FILE = os.path.join(DATA_DIR, "gaunt_factor.dat")
@@ -69,6 +69,25 @@ def camera(position, look_at, roll, screen_width, num_pix_x, num_pix_y):
     c.roll, c.screen_width = float(roll), float(screen_width)
     c.num_pix_x, c.num_pix_y = int(num_pix_x), int(num_pix_y)
     return c
+
+
+def job(cam, z_range=0.0, aperture_radius=0.0, sphere_center=(0.0, 0.0, 0.0),
+        sphere_radius=0.0, min_chord=0.0, scale=1.0, out_offset=0):
+    """One camera of a batched render (ilc_job)."""
+    return Job(cam, z_range, aperture_radius, (ctypes.c_double * 3)(*sphere_center),
+               sphere_radius, min_chord, scale, 0, out_offset)
+
+
+def pack_jobs(jobs, n_channels):
+    """Assigns consecutive output blocks (V x ny x nx each) to the jobs in
+    order; returns (ctypes array, total elements)."""
+    arr = (Job * len(jobs))()
+    off = 0
+    for i, j in enumerate(jobs):
+        j.out_offset = off
+        arr[i] = j
+        off += n_channels * j.camera.num_pix_x * j.camera.num_pix_y
+    return arr, off
 
 
 def camera_plane(cam):
@@ -122,19 +141,30 @@ class Context:
     def set_z_window(self, kpc):
         self.check(self.L.ilc_set_z_window(self.h, float(kpc)))
 
-    def autotune_z_window(self, cam, z_range, rel_tol=1e-3, abs_tol=0.0,
-                          controller=CONTROLLER_FP64, candidates=(0, 2, 5, 10, 20, 40, 80),
-                          sample_stride=16):
-        """Times the adaptive render on a sample of tile rows for each candidate
-        z window, sets the fastest on the context; returns (best, {window: ms})."""
-        cand = np.ascontiguousarray(candidates, np.float32)
-        times = np.zeros(len(cand), np.float32)
-        best = ctypes.c_float(0.0)
-        self.check(self.L.ilc_autotune_z_window(self.h, ctypes.byref(cam), float(z_range),
-                                                Tolerance(abs_tol, rel_tol), controller,
-                                                _ptr(cand), len(cand), int(sample_stride),
-                                                ctypes.byref(best), _ptr(times)))
-        return float(best.value), {float(c): float(t) for c, t in zip(cand, times)}
+    def set_render_engine(self, engine):
+        self.check(self.L.ilc_set_render_engine(self.h, int(engine)))
+
+    def set_render_occupancy(self, blocks_per_sm):
+        self.check(self.L.ilc_set_render_occupancy(self.h, int(blocks_per_sm)))
+
+    def autotune_render(self, cam, z_range, rel_tol=1e-3, abs_tol=0.0,
+                        controller=CONTROLLER_FP64, windows=(0, 5, 10, 20, 40, 80),
+                        occupancies=(0, 3, 4), sample_stride=16):
+        """Times the adaptive render on a sample of tile rows for each
+        (z window, occupancy) pair, sets the fastest on the context; returns
+        (best window, best occupancy, {(window, occupancy): ms})."""
+        win = np.ascontiguousarray(windows, np.float32)
+        occ = np.ascontiguousarray(occupancies, np.int32)
+        times = np.zeros(len(win) * len(occ), np.float32)
+        bw, bo = ctypes.c_float(0.0), ctypes.c_int32(0)
+        self.check(self.L.ilc_autotune_render(self.h, ctypes.byref(cam), float(z_range),
+                                              Tolerance(abs_tol, rel_tol), controller,
+                                              _ptr(win), len(win), _ptr(occ), len(occ),
+                                              int(sample_stride), ctypes.byref(bw),
+                                              ctypes.byref(bo), _ptr(times)))
+        tt = {(float(w), int(o)): float(times[i * len(occ) + j])
+              for i, w in enumerate(win) for j, o in enumerate(occ)}
+        return float(bw.value), int(bo.value), tt
 
     # ---- grid / nn8
     def setup_particles(self, xyzq):
@@ -215,6 +245,25 @@ class Context:
                                                           dev))
         return out
 
+    def xray_spectrum(self, rho, u, xe, energies, widths, redshift=REDSHIFT,
+                      luminosity_distance=LUMINOSITY_DISTANCE):
+        """Per-cell flux in every bin, cell-major (n, n_bins)."""
+        dev = _is_dev(u)
+        if not dev:
+            rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+        e = np.ascontiguousarray(energies, np.float32)
+        w = np.ascontiguousarray(widths, np.float32)
+        n, nb = u.shape[0], e.shape[0]
+        if dev:
+            import torch
+            out = torch.empty((n, nb), dtype=torch.float32, device=u.device)
+        else:
+            out = np.zeros((n, nb), np.float32)
+        self.check(self.L.ilc_quantity_xray_spectrum(self.h, _ptr(rho), _ptr(u), _ptr(xe), n,
+                                                     redshift, luminosity_distance, _ptr(e),
+                                                     _ptr(w), nb, _ptr(out), dev))
+        return out
+
     def mean_temperature(self, u, xe):
         _, u, xe, n, out, dev = self._q3(None, u, xe)
         self.check(self.L.ilc_quantity_temperature(self.h, _ptr(u), _ptr(xe), n, _ptr(out), dev))
@@ -282,9 +331,89 @@ class Context:
             _ptr(g_r), _ptr(g_t), 0, ctypes.byref(st)))
         return img, g_r, g_t, st.as_dict()
 
+    # ---- batched render
+    def set_batch_schedule(self, tile_w=8, blocks_per_sm=0, z_window=0.0, cost_order=True):
+        self.check(self.L.ilc_set_batch_schedule(self.h, int(tile_w), int(blocks_per_sm),
+                                                 float(z_window), 1 if cost_order else 0))
+
+    def render_batched(self, values, jobs, rel_tol=1e-3, abs_tol=0.0, images=None):
+        """values: (n,) or (n, V) per-cell channels (original particle order;
+        host array or device tensor). jobs: list of ilc_job (their out_offset
+        is assigned here, consecutively). Returns (flat images, stats); job
+        k's block is images[off_k : off_k + V*ny*nx] as (V, ny, nx)."""
+        dev = _is_dev(values)
+        if not dev:
+            values = np.ascontiguousarray(values, np.float32)
+        V = 1 if values.ndim == 1 else int(values.shape[1])
+        arr, total = pack_jobs(jobs, V)
+        if images is None:
+            if dev:
+                import torch
+                images = torch.zeros(total, dtype=torch.float32, device=values.device)
+            else:
+                images = np.zeros(total, np.float32)
+        st = RenderStats()
+        self.check(self.L.ilc_render_batched(self.h, _ptr(values), V, dev, arr, len(jobs),
+                                             Tolerance(abs_tol, rel_tol), _ptr(images), total,
+                                             _is_dev(images), ctypes.byref(st)))
+        return images, st.as_dict()
+
+    def autotune_batched(self, values, jobs, rel_tol=1e-3, abs_tol=0.0,
+                         tile_ws=(4, 8, 16, 32), occupancies=(0, 3, 4), windows=(0.0, 40.0)):
+        """Times every (tile_w, occupancy, z_window) on the jobs, sets the
+        fastest; returns (tile_w, occupancy, window, {(t, o, w): ms})."""
+        dev = _is_dev(values)
+        if not dev:
+            values = np.ascontiguousarray(values, np.float32)
+        V = 1 if values.ndim == 1 else int(values.shape[1])
+        arr, _ = pack_jobs(jobs, V)
+        tw = np.ascontiguousarray(tile_ws, np.int32)
+        oc = np.ascontiguousarray(occupancies, np.int32)
+        wn = np.ascontiguousarray(windows, np.float32)
+        times = np.zeros(len(tw) * len(oc) * len(wn), np.float32)
+        bt, bo, bw = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_float(0.0)
+        self.check(self.L.ilc_autotune_batched(self.h, _ptr(values), V, dev, arr, len(jobs),
+                                               Tolerance(abs_tol, rel_tol), _ptr(tw), len(tw),
+                                               _ptr(oc), len(oc), _ptr(wn), len(wn),
+                                               ctypes.byref(bt), ctypes.byref(bo),
+                                               ctypes.byref(bw), _ptr(times)))
+        tt = {}
+        for i, t in enumerate(tw):
+            for j, o in enumerate(oc):
+                for q, w in enumerate(wn):
+                    tt[(int(t), int(o), float(w))] = float(times[(i * len(oc) + j) * len(wn) + q])
+        return int(bt.value), int(bo.value), float(bw.value), tt
+
     @property
     def kernel_launches(self):
         return int(self.L.ilc_kernel_launches(self.h))
+
+    def render_record(self, cam, z_range, capacity, rel_tol=1e-3, abs_tol=0.0,
+                      controller=CONTROLLER_FP64):
+        """Adaptive render plus every ray's accepted step sizes:
+        (image, step_sizes (rays, capacity), n_steps (rays,), stats)."""
+        img = self._image(cam, False)
+        rays = cam.num_pix_x * cam.num_pix_y
+        hs = np.zeros((rays, capacity), np.float32)
+        n = np.zeros(rays, np.int32)
+        st = RenderStats()
+        self.check(self.L.ilc_render_record(self.h, ctypes.byref(cam), float(z_range),
+                                            Tolerance(abs_tol, rel_tol), controller, _ptr(hs),
+                                            _ptr(n), capacity, 0, _ptr(img), 0,
+                                            ctypes.byref(st)))
+        return img, hs, n, st.as_dict()
+
+    def render_frozen(self, cam, z_range, step_sizes, n_steps, scaling=None):
+        """Replays per-ray step sequences (rays x capacity), all accepted."""
+        hs = np.ascontiguousarray(step_sizes, np.float32)
+        n = np.ascontiguousarray(n_steps, np.int32)
+        img = self._image(cam, False)
+        st = RenderStats()
+        sc = None if scaling is None else ctypes.byref(scaling)
+        self.check(self.L.ilc_render_frozen(self.h, ctypes.byref(cam), float(z_range), _ptr(hs),
+                                            _ptr(n), hs.shape[1], 0, sc, _ptr(img), 0,
+                                            ctypes.byref(st)))
+        return img, st.as_dict()
 
     def render_fixed(self, cam, z_range, num_steps, scaling=None, device_output=False):
         img = self._image(cam, device_output)

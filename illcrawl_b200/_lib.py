@@ -19,6 +19,7 @@ STATUS_NAMES = {
 CONTROLLER_REF32 = 0
 CONTROLLER_FP64 = 1
 DA_PIXEL_AREA, DA_UNIT, DA_INVERSE_RANGE = 0, 1, 2
+ENGINE_GRID, ENGINE_PERSISTENT = 0, 1
 
 
 class IlcError(RuntimeError):
@@ -69,6 +70,15 @@ class AdjointStats(ctypes.Structure):
 
 ADJOINT_CHECKPOINT, ADJOINT_RECOMPUTE = 0, 1
 
+
+class Job(ctypes.Structure):
+    """ilc_job: one camera of a batched render."""
+    _fields_ = [("camera", Camera), ("z_range", ctypes.c_double),
+                ("aperture_radius", ctypes.c_double), ("sphere_center", ctypes.c_double * 3),
+                ("sphere_radius", ctypes.c_double), ("min_chord", ctypes.c_double),
+                ("scale", ctypes.c_float), ("reserved", ctypes.c_int32),
+                ("out_offset", ctypes.c_uint64)]
+
 _P = ctypes.c_void_p
 _u64, _i64, _i32, _f32, _f64, _int = (ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,
                                       ctypes.c_float, ctypes.c_double, ctypes.c_int)
@@ -94,12 +104,23 @@ SIGNATURES = {
     "ilc_camera_plane": (_int, [_P, _P]),
     "ilc_render_adaptive": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _P, _int, _P]),
     "ilc_render_fixed": (_int, [_P, _P, _f64, _i64, _P, _P, _int, _P]),
+    "ilc_render_record": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _P, _i64, _int, _P, _int, _P]),
+    "ilc_render_frozen": (_int, [_P, _P, _f64, _P, _P, _i64, _int, _P, _P, _int, _P]),
     "ilc_los_scale": (_f32, [_P, _f64, _P]),
     "ilc_project_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
                                      _f64, Tolerance, _i32, _P, _P, _int, _P]),
     "ilc_kernel_launches": (_u64, [_P]),
     "ilc_grid_build_noalloc": (_int, [_P, _u64, _P, _P, _u64, _P, _P, _P]),
-    "ilc_autotune_z_window": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _i32, _i32, _P, _P]),
+    "ilc_autotune_render": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _i32, _P, _i32, _i32, _P,
+                                   _P, _P]),
+    "ilc_set_render_occupancy": (_int, [_P, _i32]),
+    "ilc_set_render_engine": (_int, [_P, _i32]),
+    "ilc_quantity_xray_spectrum": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _P, _P, _i32, _P,
+                                          _int]),
+    "ilc_render_batched": (_int, [_P, _P, _i32, _int, _P, _i32, Tolerance, _P, _u64, _int, _P]),
+    "ilc_set_batch_schedule": (_int, [_P, _i32, _i32, _f32, _i32]),
+    "ilc_autotune_batched": (_int, [_P, _P, _i32, _int, _P, _i32, Tolerance, _P, _i32, _P, _i32,
+                                    _P, _i32, _P, _P, _P, _P]),
     "ilc_adjoint_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
                                      _f64, Tolerance, _i32, _P, _P, _i32, _P, _P, _P, _int, _P]),
 }

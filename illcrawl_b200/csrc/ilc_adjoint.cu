@@ -17,6 +17,7 @@
 #include "ilc_device.cuh"
 #include "ilc_internal.h"
 #include "ilc_quantity.cuh"
+#include "ilc_walk4.cuh"
 
 namespace ilc {
 
@@ -154,9 +155,37 @@ __global__ void loss_seed_kernel(const float* __restrict__ img, const float* __r
 }
 
 // d e / d v_p = w_p / sum(w) for the 8 slots of one evaluation (0 where the
-// finalize has no weight); adds c * that to grad at the sorted particle index.
-__device__ __forceinline__ void scatter_slots(const Slots<true>& s, float c,
-                                              float* __restrict__ grad) {
+// finalize has no weight): scatter4 adds c * that to grad at the sorted
+// particle index of point J's slots. The accumulator is double: a cell's
+// gradient sums contributions of both signs from many rays, and fp32
+// accumulation loses digits to cancellation.
+template <int J>
+__device__ __forceinline__ void scatter4(const Step4& s, float c, double* __restrict__ grad) {
+  if (c == 0.0f) return;
+  float w[8];
+  float ws = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    w[t] = weight3d(s.d[J][t]);
+    ws = ws + w[t];
+  }
+  if (!(ws > 0.0f) || !isfinite(ws)) return;
+  const double f = (double)c / (double)ws;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int id = __float_as_int(s.v[J][t]);
+    if (id >= 0 && w[t] != 0.0f) atomicAdd(&grad[id], f * (double)w[t]);
+  }
+}
+
+// Point 2's slots of the previous step (it is the next step's k1).
+struct PrevSlots {
+  float d[8];
+  int id[8];
+};
+
+__device__ __forceinline__ void scatter_prev(const PrevSlots& s, float c,
+                                             double* __restrict__ grad) {
   if (c == 0.0f) return;
   float w[8];
   float ws = 0.0f;
@@ -166,17 +195,36 @@ __device__ __forceinline__ void scatter_slots(const Slots<true>& s, float c,
     ws = ws + w[t];
   }
   if (!(ws > 0.0f) || !isfinite(ws)) return;
-  const float f = c / ws;
+  const double f = (double)c / (double)ws;
 #pragma unroll
   for (int t = 0; t < 8; ++t)
-    if (s.id[t] >= 0 && w[t] != 0.0f) atomicAdd(&grad[s.id[t]], f * w[t]);
+    if (s.id[t] >= 0 && w[t] != 0.0f) atomicAdd(&grad[s.id[t]], f * (double)w[t]);
 }
 
-__device__ __forceinline__ void walk_ids(const GridView& g, const char4* spiral, float px,
-                                         float py, float pz, float lx, float ly, float lz,
-                                         float zq, Slots<true>& s, WalkStats& st) {
-  s.init();
-  nn8_walk<true>(g, spiral, px + zq * lx, py + zq * ly, pz + zq * lz, s, st);
+__device__ __forceinline__ void keep_prev(const Step4& s, PrevSlots& p) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    p.d[t] = s.d[2][t];
+    p.id[t] = __float_as_int(s.v[2][t]);
+  }
+}
+
+// nn8 value of point J (finalize order) with the values read by index.
+template <int J>
+__device__ __forceinline__ float value_by_id(const Step4& s, const float4* __restrict__ parts) {
+  float w[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) w[t] = weight3d(s.d[J][t]);
+  float ws = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) ws = ws + w[t];
+  float dot = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int id = __float_as_int(s.v[J][t]);
+    dot = __fmaf_rn(w[t], id >= 0 ? __ldg(&parts[id].w) : 0.0f, dot);
+  }
+  return (ws != 0.0f && dot != 0.0f) ? dot / ws : 0.0f;
 }
 
 struct AdjK {
@@ -190,7 +238,7 @@ struct AdjK {
   const int32_t* __restrict__ rec_n;
   int64_t rec_cap;
   const float* __restrict__ seed;  // dL/dI_raw per pixel
-  float* __restrict__ grad;        // dL/dq per sorted particle
+  double* __restrict__ grad;       // dL/dq per sorted particle
 };
 
 __global__ void __launch_bounds__(128)
@@ -210,7 +258,7 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
   const float lx = a.cam.look0, ly = a.cam.look1, lz = a.cam.look2;
   WalkStats ws;
   unsigned long long steps = 0;
-  Slots<true> prev, s0, s1, s2;
+  PrevSlots prev;
   bool have_prev = false;
   float z = a.z0;
   if (a.mode == ILC_ADJOINT_CHECKPOINT) {
@@ -220,14 +268,13 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
       const float h = hs[i];
       float p[4];
       rkf_points(z, h, p);
-      walk_ids(g, spiral, px, py, pz, lx, ly, lz, p[0], s0, ws);
-      walk_ids(g, spiral, px, py, pz, lx, ly, lz, p[1], s1, ws);
-      walk_ids(g, spiral, px, py, pz, lx, ly, lz, p[2], s2, ws);
-      scatter_slots(s0, gi * (h * 1408.f / 2565.f), a.grad);
-      scatter_slots(s1, gi * (h * 2197.f / 4101.f), a.grad);
-      scatter_slots(s2, gi * (-h / 5.f), a.grad);
-      if (have_prev) scatter_slots(prev, gi * (h * 25.f / 216.f), a.grad);
-      prev = s2;
+      Step4 s;
+      nn8_walk_step4<true>(g, spiral, px, py, pz, lx, ly, lz, p, s, ws);
+      scatter4<0>(s, gi * (h * 1408.f / 2565.f), a.grad);
+      scatter4<1>(s, gi * (h * 2197.f / 4101.f), a.grad);
+      scatter4<2>(s, gi * (-h / 5.f), a.grad);
+      if (have_prev) scatter_prev(prev, gi * (h * 25.f / 216.f), a.grad);
+      keep_prev(s, prev);
       have_prev = true;
       z += h;
       ++steps;
@@ -238,15 +285,12 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
     float pts[4];
     rkf_points(z, h, pts);
     const float fa = (float)a.atol, fr = (float)a.rtol;
-    Slots<true> s3;
     while (z < a.z_end) {
       if ((int64_t)steps >= a.max_steps) { atomicOr(flags, FLAG_STEP_LIMIT); break; }
-      walk_ids(g, spiral, px, py, pz, lx, ly, lz, pts[0], s0, ws);
-      walk_ids(g, spiral, px, py, pz, lx, ly, lz, pts[1], s1, ws);
-      walk_ids(g, spiral, px, py, pz, lx, ly, lz, pts[2], s2, ws);
-      walk_ids(g, spiral, px, py, pz, lx, ly, lz, pts[3], s3, ws);
-      const float e[4] = {nn8_finalize(s0), nn8_finalize(s1), nn8_finalize(s2),
-                          nn8_finalize(s3)};
+      Step4 s;
+      nn8_walk_step4<true>(g, spiral, px, py, pz, lx, ly, lz, pts, s, ws);
+      const float e[4] = {value_by_id<0>(s, g.parts), value_by_id<1>(s, g.parts),
+                          value_by_id<2>(s, g.parts), value_by_id<3>(s, g.parts)};
       const float zb = z, hb = h;
       if (a.controller == ILC_CONTROLLER_REF32)
         rkf_advance_ref32(I, z, h, k1, fa, fr, a.z_end, e, kEps, kHmin, kHmax, pts);
@@ -254,11 +298,11 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
         rkf_advance_fp64(I, z, h, k1, a.atol, a.rtol, a.z_end, e, kEps, kHmin, kHmax, pts);
       ++steps;
       if (z != zb) {
-        scatter_slots(s0, gi * (hb * 1408.f / 2565.f), a.grad);
-        scatter_slots(s1, gi * (hb * 2197.f / 4101.f), a.grad);
-        scatter_slots(s2, gi * (-hb / 5.f), a.grad);
-        if (have_prev) scatter_slots(prev, gi * (hb * 25.f / 216.f), a.grad);
-        prev = s2;
+        scatter4<0>(s, gi * (hb * 1408.f / 2565.f), a.grad);
+        scatter4<1>(s, gi * (hb * 2197.f / 4101.f), a.grad);
+        scatter4<2>(s, gi * (-hb / 5.f), a.grad);
+        if (have_prev) scatter_prev(prev, gi * (hb * 25.f / 216.f), a.grad);
+        keep_prev(s, prev);
         have_prev = true;
       }
     }
@@ -270,7 +314,7 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
 }
 
 // dL/dln rho and dL/dln T in the original particle order.
-__global__ void cell_grad_kernel(const float* __restrict__ grad_sorted,
+__global__ void cell_grad_kernel(const double* __restrict__ grad_sorted,
                                  const uint32_t* __restrict__ s2u, uint64_t n,
                                  const float* __restrict__ dq_lnrho,
                                  const float* __restrict__ dq_lnT, float* __restrict__ g_lnrho,
@@ -278,9 +322,9 @@ __global__ void cell_grad_kernel(const float* __restrict__ grad_sorted,
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t o = s2u[i];
-  const float gq = grad_sorted[i];
-  g_lnrho[o] = gq * dq_lnrho[o];
-  g_lnT[o] = gq * dq_lnT[o];
+  const double gq = grad_sorted[i];
+  g_lnrho[o] = (float)(gq * (double)dq_lnrho[o]);
+  g_lnT[o] = (float)(gq * (double)dq_lnT[o]);
 }
 
 }  // namespace
@@ -311,7 +355,7 @@ cudaError_t adjoint_seed_launch(Context& c, const float* img, const float* targe
 }
 
 cudaError_t adjoint_ray_launch(Context& c, const RenderArgs& r, int mode, const float* seed,
-                               float* grad, float* kernel_ms) {
+                               double* grad, float* kernel_ms) {
   cudaError_t e;
   if ((e = c.flags.ensure(kFlagsBytes))) return e;
   if ((e = cudaMemsetAsync(c.flags.p, 0, kFlagsBytes, c.stream))) return e;
@@ -351,7 +395,7 @@ cudaError_t adjoint_ray_launch(Context& c, const RenderArgs& r, int mode, const 
   return cudaSuccess;
 }
 
-cudaError_t adjoint_chain_launch(Context& c, const float* grad, uint64_t n, const float* dq_lnrho,
+cudaError_t adjoint_chain_launch(Context& c, const double* grad, uint64_t n, const float* dq_lnrho,
                                  const float* dq_lnT, float* g_lnrho, float* g_lnT) {
   ++c.launches;
   cell_grad_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "ilc_internal.h"
 
@@ -92,7 +93,7 @@ void make_grid_params(const float mn_f[3], const float mx_f[3], uint64_t n, Grid
 
 // camera::update_basis_vectors / update_min_position (camera.cpp:124-155,
 // math.hpp:85-149), in double, then cast to float.
-void camera_plane(const ilc_camera& cam, float out[13]) {
+void camera_plane(const ilc_camera& cam, float out[13], double* outd = nullptr) {
   auto dot3 = [](const double* a, const double* b) {
     double r = 0.0;
     for (int i = 0; i < 3; ++i) r += a[i] * b[i];
@@ -133,6 +134,15 @@ void camera_plane(const ilc_camera& cam, float out[13]) {
     out[9 + i] = (float)mp[i];
   }
   out[12] = (float)ps;
+  if (outd) {
+    for (int i = 0; i < 3; ++i) {
+      outd[i] = cam.look_at[i];
+      outd[3 + i] = b0[i];
+      outd[6 + i] = b1[i];
+      outd[9 + i] = mp[i];
+    }
+    outd[12] = ps;
+  }
 }
 
 float los_scale(const ilc_camera& cam, double z_range, const ilc_los_scaling& s) {
@@ -189,15 +199,118 @@ ilc_status build_grid_staged(Context& c, uint64_t n) {
   return ILC_OK;
 }
 
+// Job table of a batched render on the device (values not staged).
+ilc_status batched_jobs(Context& c, int32_t V, const ilc_job* jobs, int32_t n_jobs,
+                        ilc_tolerance tol, uint64_t images_len, BatchArgs* a) {
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "batched render before setup_particles");
+  if (V < 1 || V > 256 || !jobs || n_jobs < 1)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid batched render arguments (1 <= V <= 256)");
+  if (!(tol.absolute >= 0.0) || !(tol.relative >= 0.0) ||
+      (tol.absolute <= 0.0 && tol.relative <= 0.0))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT,
+                "either the absolute or the relative tolerance has to be > 0");
+  std::vector<JobDev> jd((size_t)n_jobs);
+  const int tw = c.batch_tile_w, th = 32 / c.batch_tile_w;
+  uint64_t items = 0;
+  for (int32_t k = 0; k < n_jobs; ++k) {
+    const ilc_job& j = jobs[k];
+    if (!camera_ok(&j.camera)) return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid job camera");
+    const bool chord = j.sphere_radius > 0.0;
+    if (!std::isfinite(j.aperture_radius) || !std::isfinite(j.sphere_radius) ||
+        !std::isfinite(j.min_chord) || !std::isfinite(j.sphere_center[0]) ||
+        !std::isfinite(j.sphere_center[1]) || !std::isfinite(j.sphere_center[2]) ||
+        (!chord && !(j.z_range > 0.0 && std::isfinite(j.z_range))))
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid job range, chord or aperture");
+    const uint64_t plane = (uint64_t)j.camera.num_pix_x * (uint64_t)j.camera.num_pix_y;
+    if (j.out_offset > images_len || (uint64_t)V * plane > images_len - j.out_offset)
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "job output block beyond images_len");
+    JobDev& d = jd[k];
+    std::memset(&d, 0, sizeof(d));
+    float f[13];
+    double dd[13];
+    camera_plane(j.camera, f, dd);
+    for (int i = 0; i < 3; ++i) {
+      d.look[i] = f[i];
+      d.b0[i] = f[3 + i];
+      d.b1[i] = f[6 + i];
+      d.minp[i] = f[9 + i];
+      d.look_d[i] = dd[i];
+      d.b0_d[i] = dd[3 + i];
+      d.b1_d[i] = dd[6 + i];
+      d.minp_d[i] = dd[9 + i];
+      d.centre[i] = j.sphere_center[i];
+    }
+    d.ps = f[12];
+    d.ps_d = dd[12];
+    d.nx = j.camera.num_pix_x;
+    d.ny = j.camera.num_pix_y;
+    d.tiles_x = (d.nx + tw - 1) / tw;
+    d.z_range = j.z_range;
+    d.aperture = j.aperture_radius;
+    d.radius = j.sphere_radius;
+    d.min_chord = j.min_chord;
+    d.scale = j.scale;
+    d.out_offset = j.out_offset;
+    d.item_begin = items;
+    items += (uint64_t)d.tiles_x * (uint64_t)((d.ny + th - 1) / th);
+  }
+  ILC_CUDA(c, c.jobs.ensure(jd.size() * sizeof(JobDev)), "job table");
+  ILC_CUDA(c, cudaMemcpyAsync(c.jobs.p, jd.data(), jd.size() * sizeof(JobDev),
+                              cudaMemcpyHostToDevice, c.stream), "job table H2D");
+  a->jobs = c.jobs.as<JobDev>();
+  a->n_jobs = n_jobs;
+  a->n_items = items;
+  a->V = V;
+  a->chan = nullptr;
+  a->atol = tol.absolute;
+  a->rtol = tol.relative;
+  a->tile_w = c.batch_tile_w;
+  a->occupancy = c.batch_occupancy;
+  a->window = c.batch_window;
+  a->order = nullptr;
+  if (c.batch_cost_order) ILC_CUDA(c, batched_order(c, *a, jd), "work order");
+  return ILC_OK;
+}
+
+// Job table plus the sorted channel table of a batched render.
+ilc_status batched_prepare(Context& c, const float* values, int32_t V, int values_on_device,
+                           const ilc_job* jobs, int32_t n_jobs, ilc_tolerance tol,
+                           uint64_t images_len, BatchArgs* a) {
+  if (!values) return fail(c, ILC_ERR_INVALID_ARGUMENT, "values is NULL");
+  ilc_status st = batched_jobs(c, V, jobs, n_jobs, tol, images_len, a);
+  if (st) return st;
+  const uint64_t n = c.n_particles;
+  const void* dv = nullptr;
+  ILC_CUDA(c, stage_in(c, c.in_a, values, n * (uint64_t)V * 4, values_on_device, &dv),
+           "values H2D");
+  ILC_CUDA(c, c.chan_sorted.ensure(n * (uint64_t)V * 4), "channel table");
+  ILC_CUDA(c, channels_sort_launch(c, static_cast<const float*>(dv), n, V,
+                                   c.chan_sorted.as<float>()), "channel sort");
+  a->chan = c.chan_sorted.as<float>();
+  return ILC_OK;
+}
+
+bool tile_w_ok(int32_t w) { return w == 1 || w == 2 || w == 4 || w == 8 || w == 16 || w == 32; }
+
+// Optional frozen replay (replay_h/replay_n) or step recording (rec_h/rec_n),
+// both device arrays of cap steps per ray; either forces the grid kernel.
+struct StepArrays {
+  const float* replay_h = nullptr;
+  const int32_t* replay_n = nullptr;
+  float* rec_h = nullptr;
+  int32_t* rec_n = nullptr;
+  int64_t cap = 0;
+};
+
 ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_tolerance tol,
                          int32_t controller, int64_t fixed_steps,
                          const ilc_los_scaling* scaling, float* image, int is_device,
-                         ilc_render_stats* stats) {
+                         ilc_render_stats* stats, const StepArrays& sa = StepArrays()) {
   if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "render before setup_particles");
   if (!camera_ok(cam)) return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid camera");
   if (!(z_range > 0.0) || !std::isfinite(z_range) || !image)
     return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z_range or image");
-  if (fixed_steps <= 0) {
+  if (fixed_steps <= 0 && !sa.replay_h) {
     if (!(tol.absolute >= 0.0) || !(tol.relative >= 0.0) ||
         (tol.absolute <= 0.0 && tol.relative <= 0.0))
       return fail(c, ILC_ERR_INVALID_ARGUMENT,
@@ -218,12 +331,31 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
   a.fixed_h = fixed_steps > 0 ? (float)(z_range / (double)fixed_steps) : 0.0f;
   a.apply_scale = scaling != nullptr;
   a.scale = scaling ? los_scale(*cam, z_range, *scaling) : 1.0f;
+  a.replay_h = sa.replay_h;
+  a.replay_n = sa.replay_n;
+  a.rec_h = sa.rec_h;
+  a.rec_n = sa.rec_n;
+  a.rec_cap = sa.cap;
   const size_t bytes = (size_t)a.nx * (size_t)a.ny * 4;
   void* dimg = nullptr;
   ILC_CUDA(c, out_ptr(c.out_a, image, bytes, is_device, &dimg), "image buffer");
   a.out = static_cast<float*>(dimg);
   float ms = 0.0f;
-  ILC_CUDA(c, render_launch(c, a, &ms), "render kernel");
+  if (c.render_engine == ILC_ENGINE_PERSISTENT && fixed_steps <= 0 &&
+      controller == ILC_CONTROLLER_FP64 && !sa.replay_h && !sa.rec_h) {
+    // one job through the persistent work-queue kernel, values = particle q
+    ilc_job j{};
+    j.camera = *cam;
+    j.z_range = z_range;
+    j.scale = a.scale;
+    BatchArgs ba{};
+    ilc_status st = batched_jobs(c, 1, &j, 1, tol, (uint64_t)a.nx * (uint64_t)a.ny, &ba);
+    if (st) return st;
+    ba.out = a.out;
+    ILC_CUDA(c, batched_launch(c, ba, &ms), "render kernel (persistent)");
+  } else {
+    ILC_CUDA(c, render_launch(c, a, &ms), "render kernel");
+  }
   ILC_CUDA(c, finish_out(c, image, dimg, bytes, is_device), "render");
   uint32_t flags = 0;
   DevStats ds{};
@@ -241,6 +373,8 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
   }
   if (flags & FLAG_STEP_LIMIT)
     return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the per-ray step limit");
+  if (flags & FLAG_REC_OVERFLOW)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "step recording capacity too small");
   return ILC_OK;
 }
 
@@ -288,8 +422,10 @@ void ilc_destroy(ilc_ctx* h) {
                     &c.hist, &c.tmp_in, &c.gaunt, &c.list_d, &c.list_v, &c.list_id, &c.in_a,
                     &c.in_b, &c.in_c, &c.out_a, &c.out_b, &c.out_c, &c.spiral, &c.flags,
                     &c.rec_h, &c.rec_n, &c.adj_dT, &c.adj_dR, &c.adj_grad, &c.adj_seed,
-                    &c.adj_loss})
+                    &c.adj_loss, &c.codes, &c.jobs, &c.chan_sorted, &c.chan_state, &c.queue,
+                    &c.item_cost, &c.item_order})
     b->release();
+  if (c.batch_exec) cudaGraphExecDestroy(c.batch_exec);
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
@@ -306,6 +442,22 @@ ilc_status ilc_set_step_limit(ilc_ctx* h, int64_t max_steps) {
 }
 
 void* ilc_get_stream(ilc_ctx* h) { return h ? (void*)h->c.stream : nullptr; }
+
+ilc_status ilc_set_render_engine(ilc_ctx* h, int32_t engine) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  if (engine != ILC_ENGINE_GRID && engine != ILC_ENGINE_PERSISTENT)
+    return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "unknown render engine");
+  h->c.render_engine = engine;
+  return ILC_OK;
+}
+
+ilc_status ilc_set_render_occupancy(ilc_ctx* h, int32_t blocks_per_sm) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  if (blocks_per_sm != 0 && blocks_per_sm != 3 && blocks_per_sm != 4)
+    return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3 or 4");
+  h->c.render_occupancy = blocks_per_sm;
+  return ILC_OK;
+}
 
 ilc_status ilc_set_z_window(ilc_ctx* h, float z_window) {
   if (!h) return ILC_ERR_INVALID_ARGUMENT;
@@ -531,6 +683,61 @@ ilc_status ilc_render_fixed(ilc_ctx* h, const ilc_camera* cam, double z_range, i
                        num_steps, scaling, image, is_device, stats);
 }
 
+ilc_status ilc_render_record(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                             ilc_tolerance tol, int32_t controller, float* step_sizes,
+                             int32_t* n_steps, int64_t capacity, int steps_on_device,
+                             float* image, int is_device, ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!camera_ok(cam) || !step_sizes || !n_steps || capacity <= 0)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid step recording arguments");
+  const uint64_t rays = (uint64_t)cam->num_pix_x * (uint64_t)cam->num_pix_y;
+  void *dh = nullptr, *dn = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_b, step_sizes, rays * (uint64_t)capacity * 4, steps_on_device, &dh),
+           "step buffer");
+  ILC_CUDA(c, out_ptr(c.out_c, n_steps, rays * 4, steps_on_device, &dn), "step counts");
+  StepArrays sa;
+  sa.rec_h = static_cast<float*>(dh);
+  sa.rec_n = static_cast<int32_t*>(dn);
+  sa.cap = capacity;
+  ilc_status st = render_common(c, cam, z_range, tol, controller, 0, nullptr, image, is_device,
+                                stats, sa);
+  ILC_CUDA(c, finish_out(c, step_sizes, dh, rays * (uint64_t)capacity * 4, steps_on_device),
+           "step buffer D2H");
+  ILC_CUDA(c, finish_out(c, n_steps, dn, rays * 4, steps_on_device), "step counts D2H");
+  return st;
+}
+
+ilc_status ilc_render_frozen(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                             const float* step_sizes, const int32_t* n_steps, int64_t capacity,
+                             int steps_on_device, const ilc_los_scaling* scaling, float* image,
+                             int is_device, ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!camera_ok(cam) || !step_sizes || !n_steps || capacity <= 0)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid frozen sequence arguments");
+  const uint64_t rays = (uint64_t)cam->num_pix_x * (uint64_t)cam->num_pix_y;
+  std::vector<int32_t> hn;
+  if (!steps_on_device) {  // a count beyond capacity would read past the ray's row
+    hn.assign(n_steps, n_steps + rays);
+    for (int32_t v : hn)
+      if (v < 0 || v > capacity)
+        return fail(c, ILC_ERR_INVALID_ARGUMENT, "n_steps outside [0, capacity]");
+  }
+  const void *dh = nullptr, *dn = nullptr;
+  ILC_CUDA(c, stage_in(c, c.in_b, step_sizes, rays * (uint64_t)capacity * 4, steps_on_device,
+                       &dh), "steps H2D");
+  ILC_CUDA(c, stage_in(c, c.in_c, n_steps, rays * 4, steps_on_device, &dn), "counts H2D");
+  StepArrays sa;
+  sa.replay_h = static_cast<const float*>(dh);
+  sa.replay_n = static_cast<const int32_t*>(dn);
+  sa.cap = capacity;
+  return render_common(c, cam, z_range, ilc_tolerance{0.0, 0.0}, ILC_CONTROLLER_REF32, 0,
+                       scaling, image, is_device, stats, sa);
+}
+
 float ilc_los_scale(const ilc_camera* cam, double z_range, const ilc_los_scaling* scaling) {
   if (!camera_ok(cam) || !scaling) return 0.0f;
   return los_scale(*cam, z_range, *scaling);
@@ -658,10 +865,10 @@ ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rh
                                   c.adj_seed.as<float>(), c.adj_loss.as<double>()),
            "loss kernel");
   // 5. adjoint rays
-  ILC_CUDA(c, c.adj_grad.ensure(n * 4), "gradient");
-  ILC_CUDA(c, cudaMemsetAsync(c.adj_grad.p, 0, n * 4, c.stream), "gradient");
+  ILC_CUDA(c, c.adj_grad.ensure(n * 8), "gradient");
+  ILC_CUDA(c, cudaMemsetAsync(c.adj_grad.p, 0, n * 8, c.stream), "gradient");
   float adj_ms = 0.0f;
-  ILC_CUDA(c, adjoint_ray_launch(c, ra, mode, c.adj_seed.as<float>(), c.adj_grad.as<float>(),
+  ILC_CUDA(c, adjoint_ray_launch(c, ra, mode, c.adj_seed.as<float>(), c.adj_grad.as<double>(),
                                  &adj_ms),
            "adjoint kernel");
   DevStats as{};
@@ -672,7 +879,7 @@ ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rh
   void *gr = nullptr, *gt = nullptr;
   ILC_CUDA(c, out_ptr(c.out_a, dL_dlnrho, n * 4, is_device, &gr), "dL/dlnrho");
   ILC_CUDA(c, out_ptr(c.out_c, dL_dlnT, n * 4, is_device, &gt), "dL/dlnT");
-  ILC_CUDA(c, adjoint_chain_launch(c, c.adj_grad.as<float>(), n, c.adj_dR.as<float>(),
+  ILC_CUDA(c, adjoint_chain_launch(c, c.adj_grad.as<double>(), n, c.adj_dR.as<float>(),
                                    c.adj_dT.as<float>(), static_cast<float*>(gr),
                                    static_cast<float*>(gt)),
            "chain rule kernel");
@@ -700,16 +907,17 @@ ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rh
   return ILC_OK;
 }
 
-ilc_status ilc_autotune_z_window(ilc_ctx* h, const ilc_camera* cam, double z_range,
-                                 ilc_tolerance tol, int32_t controller, const float* candidates,
-                                 int32_t n_candidates, int32_t sample_stride, float* best,
-                                 float* times_ms) {
+ilc_status ilc_autotune_render(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                               ilc_tolerance tol, int32_t controller, const float* windows,
+                               int32_t n_windows, const int32_t* occupancies,
+                               int32_t n_occupancies, int32_t sample_stride, float* best_window,
+                               int32_t* best_occupancy, float* times_ms) {
   if (!h) return ILC_ERR_INVALID_ARGUMENT;
   Context& c = h->c;
   cudaSetDevice(c.device);
   if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "autotune before setup_particles");
-  if (!camera_ok(cam) || !candidates || n_candidates <= 0 || sample_stride <= 0 || !best ||
-      !(z_range > 0.0))
+  if (!camera_ok(cam) || !windows || n_windows <= 0 || !occupancies || n_occupancies <= 0 ||
+      sample_stride <= 0 || !best_window || !best_occupancy || !(z_range > 0.0))
     return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid autotune arguments");
   RenderArgs a{};
   camera_plane(*cam, a.cam);
@@ -726,24 +934,202 @@ ilc_status ilc_autotune_z_window(ilc_ctx* h, const ilc_camera* cam, double z_ran
   ILC_CUDA(c, c.out_b.ensure((size_t)a.nx * (size_t)a.ny * 4), "autotune image");
   a.out = c.out_b.as<float>();
   float best_ms = 0.0f;
-  for (int32_t i = 0; i < n_candidates; ++i) {
-    if (!(candidates[i] >= 0.0f) || !std::isfinite(candidates[i]))
+  bool first = true;
+  for (int32_t i = 0; i < n_windows; ++i) {
+    if (!(windows[i] >= 0.0f) || !std::isfinite(windows[i]))
       return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z window candidate");
-    a.window_override = candidates[i];
-    float ms = 0.0f;
-    ILC_CUDA(c, render_launch(c, a, &ms), "autotune render");
-    uint32_t flags = 0;
-    ilc_status st = read_flags(c, &flags, nullptr);
-    if (st) return st;
-    if (flags & FLAG_STEP_LIMIT)
-      return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the per-ray step limit");
-    if (times_ms) times_ms[i] = ms;
-    if (i == 0 || ms < best_ms) {
-      best_ms = ms;
-      *best = candidates[i];
+    for (int32_t j = 0; j < n_occupancies; ++j) {
+      if (occupancies[j] != 0 && occupancies[j] != 3 && occupancies[j] != 4)
+        return fail(c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3 or 4");
+      a.window_override = windows[i];
+      a.occupancy_override = occupancies[j];
+      float ms = 0.0f;
+      ILC_CUDA(c, render_launch(c, a, &ms), "autotune render");
+      uint32_t flags = 0;
+      ilc_status st = read_flags(c, &flags, nullptr);
+      if (st) return st;
+      if (flags & FLAG_STEP_LIMIT)
+        return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the per-ray step limit");
+      if (times_ms) times_ms[i * n_occupancies + j] = ms;
+      if (first || ms < best_ms) {
+        first = false;
+        best_ms = ms;
+        *best_window = windows[i];
+        *best_occupancy = occupancies[j];
+      }
     }
   }
-  c.z_window = *best;
+  c.z_window = *best_window;
+  c.render_occupancy = *best_occupancy;
+  return ILC_OK;
+}
+
+
+ilc_status ilc_quantity_xray_spectrum(ilc_ctx* h, const float* rho, const float* u,
+                                      const float* xe, uint64_t n, float redshift,
+                                      float luminosity_distance, const float* energies,
+                                      const float* widths, int32_t n_bins, float* out,
+                                      int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (n == 0) return ILC_OK;
+  if (!rho || !u || !xe || !out || !energies || !widths || n_bins < 1)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid xray_spectrum arguments");
+  const float *a, *b, *d;
+  ilc_status st = quantity_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  std::vector<float> ed(2 * (size_t)n_bins);
+  std::memcpy(ed.data(), energies, 4 * (size_t)n_bins);
+  std::memcpy(ed.data() + n_bins, widths, 4 * (size_t)n_bins);
+  ILC_CUDA(c, c.out_c.ensure(8 * (size_t)n_bins), "bin table");
+  ILC_CUDA(c, cudaMemcpyAsync(c.out_c.p, ed.data(), 8 * (size_t)n_bins, cudaMemcpyHostToDevice,
+                              c.stream), "bin table H2D");
+  void* dout = nullptr;
+  const size_t bytes = n * (size_t)n_bins * 4;
+  ILC_CUDA(c, out_ptr(c.out_a, out, bytes, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_xray_bins_launch(c, a, b, d, n, redshift, luminosity_distance,
+                                        c.out_c.as<float>(), c.out_c.as<float>() + n_bins,
+                                        n_bins, static_cast<float*>(dout)),
+           "xray_spectrum kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, bytes, is_device), "xray_spectrum");
+  return ILC_OK;
+}
+
+ilc_status ilc_set_batch_schedule(ilc_ctx* h, int32_t tile_w, int32_t blocks_per_sm,
+                                  float z_window, int32_t cost_order) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  if (!tile_w_ok(tile_w) || (blocks_per_sm != 0 && blocks_per_sm != 3 && blocks_per_sm != 4) ||
+      !(z_window >= 0.0f) || !std::isfinite(z_window))
+    return fail(h->c, ILC_ERR_INVALID_ARGUMENT,
+                "tile_w in 1..32 (powers of 2), occupancy 0, 3 or 4, z_window >= 0");
+  h->c.batch_tile_w = tile_w;
+  h->c.batch_occupancy = blocks_per_sm;
+  h->c.batch_window = z_window;
+  h->c.batch_cost_order = cost_order != 0;
+  return ILC_OK;
+}
+
+ilc_status ilc_render_batched(ilc_ctx* h, const float* values, int32_t n_channels,
+                              int values_on_device, const ilc_job* jobs, int32_t n_jobs,
+                              ilc_tolerance tol, float* images, uint64_t images_len,
+                              int images_on_device, ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!images || images_len == 0)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid images buffer");
+  BatchArgs a{};
+  ilc_status st = batched_prepare(c, values, n_channels, values_on_device, jobs, n_jobs, tol,
+                                  images_len, &a);
+  if (st) return st;
+  void* dimg = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_b, images, images_len * 4, images_on_device, &dimg), "images");
+  a.out = static_cast<float*>(dimg);
+  float ms = 0.0f;
+  ILC_CUDA(c, batched_launch(c, a, &ms), "batched render kernel");
+  ILC_CUDA(c, finish_out(c, images, dimg, images_len * 4, images_on_device), "batched render");
+  uint32_t flags = 0;
+  DevStats ds{};
+  st = read_flags(c, &flags, &ds);
+  if (st) return st;
+  if (stats) {
+    stats->steps = ds.steps;
+    stats->accepted_steps = ds.accepted;
+    stats->queries = ds.queries;
+    stats->cells_visited = ds.cells;
+    stats->candidates = ds.cands;
+    stats->max_steps_per_ray = ds.max_steps;
+    stats->rays_at_step_limit = ds.rays_at_limit;
+    stats->kernel_ms = ms;
+  }
+  if (flags & FLAG_STEP_LIMIT)
+    return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the per-ray step limit");
+  return ILC_OK;
+}
+
+ilc_status ilc_autotune_batched(ilc_ctx* h, const float* values, int32_t n_channels,
+                                int values_on_device, const ilc_job* jobs, int32_t n_jobs,
+                                ilc_tolerance tol, const int32_t* tile_ws, int32_t n_tiles,
+                                const int32_t* occupancies, int32_t n_occupancies,
+                                const float* windows, int32_t n_windows, int32_t* best_tile_w,
+                                int32_t* best_occupancy, float* best_window, float* times_ms) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!tile_ws || n_tiles < 1 || !occupancies || n_occupancies < 1 || !windows ||
+      n_windows < 1 || !best_tile_w || !best_occupancy || !best_window || !jobs || n_jobs < 1)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid autotune arguments");
+  for (int32_t i = 0; i < n_tiles; ++i)
+    if (!tile_w_ok(tile_ws[i])) return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid tile_w");
+  for (int32_t i = 0; i < n_occupancies; ++i)
+    if (occupancies[i] != 0 && occupancies[i] != 3 && occupancies[i] != 4)
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3 or 4");
+  for (int32_t i = 0; i < n_windows; ++i)
+    if (!(windows[i] >= 0.0f) || !std::isfinite(windows[i]))
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z window");
+  uint64_t len = 0;
+  for (int32_t k = 0; k < n_jobs; ++k) {
+    const uint64_t e = jobs[k].out_offset + (uint64_t)n_channels *
+                                                (uint64_t)jobs[k].camera.num_pix_x *
+                                                (uint64_t)jobs[k].camera.num_pix_y;
+    len = std::max(len, e);
+  }
+  const int32_t keep_w = c.batch_tile_w, keep_o = c.batch_occupancy;
+  const float keep_z = c.batch_window;
+  const bool keep_order = c.batch_cost_order;
+  auto restore = [&]() {
+    c.batch_tile_w = keep_w;
+    c.batch_occupancy = keep_o;
+    c.batch_window = keep_z;
+    c.batch_cost_order = keep_order;
+  };
+  float best = 0.0f;
+  bool first = true;
+  for (int32_t i = 0; i < n_tiles; ++i) {
+    for (int32_t j = 0; j < n_occupancies; ++j) {
+      for (int32_t q = 0; q < n_windows; ++q) {
+        c.batch_tile_w = tile_ws[i];
+        c.batch_occupancy = occupancies[j];
+        c.batch_window = windows[q];
+        c.batch_cost_order = true;
+        BatchArgs a{};
+        ilc_status st = batched_prepare(c, values, n_channels, values_on_device, jobs, n_jobs,
+                                        tol, len, &a);
+        if (st) {
+          restore();
+          return st;
+        }
+        ILC_CUDA(c, c.out_b.ensure(len * 4), "autotune images");
+        a.out = c.out_b.as<float>();
+        float ms = 0.0f;
+        ILC_CUDA(c, batched_launch(c, a, &ms), "autotune batched kernel");
+        uint32_t flags = 0;
+        st = read_flags(c, &flags, nullptr);
+        if (st) {
+          restore();
+          return st;
+        }
+        if (flags & FLAG_STEP_LIMIT) {
+          restore();
+          return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the per-ray step limit");
+        }
+        if (times_ms) times_ms[(i * n_occupancies + j) * n_windows + q] = ms;
+        if (first || ms < best) {
+          first = false;
+          best = ms;
+          *best_tile_w = tile_ws[i];
+          *best_occupancy = occupancies[j];
+          *best_window = windows[q];
+        }
+      }
+    }
+  }
+  c.batch_tile_w = *best_tile_w;
+  c.batch_occupancy = *best_occupancy;
+  c.batch_window = *best_window;
+  c.batch_cost_order = true;
   return ILC_OK;
 }
 

@@ -84,6 +84,11 @@ struct GridView {
   int n0, n1, n2;             // cells per axis
   const int2* __restrict__ cells;     // [begin, end) per cell
   const float4* __restrict__ parts;   // (x, y, z, q) in cell order
+  // Sub-box codes for exact candidate pruning: per sorted particle one byte,
+  // sx + 4 sy + 16 sz, its quarter of the cell per axis (4 per word).
+  const uint32_t* __restrict__ codes;
+  float inv_w0, inv_w1, inv_w2;       // 4 / cell size
+  float margin;                       // slack covering float rounding (cell size / 1024)
 };
 
 // Per-thread walk statistics (algorithmic traffic accounting).

@@ -217,6 +217,32 @@ __global__ void cell_ranges_kernel(const uint32_t* __restrict__ sk, uint64_t n,
   if (i + 1 == n || sk[i + 1] != k) cells[k].y = (int)(i + 1);
 }
 
+// Sub-box code of every sorted particle: which quarter of its cell it lies in
+// per axis (clamped to 0..3), packed sx + 4 sy + 16 sz. The nn8 walk uses it
+// only to skip candidates that lie, by more than a rounding margin, outside
+// the cube of the current search radius around the query points: those could
+// never be inserted, so skipping them leaves every result unchanged.
+__global__ void codes_kernel(const float4* __restrict__ parts, const uint32_t* __restrict__ sk,
+                             uint64_t n, KeyGrid kg, uint8_t* __restrict__ codes) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t k = sk[i];
+  const uint32_t kx = k % (uint32_t)kg.n0, kyz = k / (uint32_t)kg.n0;
+  const uint32_t ky = kyz % (uint32_t)kg.n1, kz = kyz / (uint32_t)kg.n1;
+  const float4 p = parts[i];
+  const float c[3] = {p.x, p.y, p.z};
+  const float mn[3] = {kg.min0 + (float)kx * kg.cs0, kg.min1 + (float)ky * kg.cs1,
+                       kg.min2 + (float)kz * kg.cs2};
+  const float iw[3] = {4.0f / kg.cs0, 4.0f / kg.cs1, 4.0f / kg.cs2};
+  int q[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float t = (c[a] - mn[a]) * iw[a];
+    q[a] = t > 0.0f ? min((int)t, 3) : 0;
+  }
+  codes[i] = (uint8_t)(q[0] | (q[1] << 2) | (q[2] << 4));
+}
+
 inline unsigned grid_blocks(uint64_t n, int threads) {
   return (unsigned)((n + threads - 1) / threads);
 }
@@ -257,7 +283,8 @@ cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n) {
   if ((e = c.keys_a.ensure(n * 4)) || (e = c.keys_b.ensure(n * 4)) ||
       (e = c.vals_a.ensure(n * 4)) || (e = c.vals_b.ensure(n * 4)) ||
       (e = c.parts.ensure(n * 16)) || (e = c.s2u.ensure(n * 4)) ||
-      (e = c.cells.ensure(g.total * 8)) || (e = c.flags.ensure(kFlagsBytes)))
+      (e = c.codes.ensure(((n + 3) / 4) * 4 + 16)) || (e = c.cells.ensure(g.total * 8)) ||
+      (e = c.flags.ensure(kFlagsBytes)))
     return e;
   const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
   if ((e = c.hist.ensure(tiles * 256 * 4 + 64))) return e;
@@ -286,9 +313,12 @@ cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n) {
   }
   gather_kernel<<<grid_blocks(n, 256), 256, 0, c.stream>>>(in, va, n, c.parts.as<float4>(),
                                                             c.s2u.as<uint32_t>());
+  c.sorted_keys = ka;
   if ((e = cudaMemsetAsync(c.cells.p, 0, g.total * 8, c.stream))) return e;
   cell_ranges_kernel<<<grid_blocks(n, 256), 256, 0, c.stream>>>(ka, n, c.cells.as<int2>());
-  c.launches += 3;  // keys, gather, cell ranges
+  codes_kernel<<<grid_blocks(n, 256), 256, 0, c.stream>>>(c.parts.as<float4>(), ka, n, kg,
+                                                           c.codes.as<uint8_t>());
+  c.launches += 4;  // keys, gather, cell ranges, codes
   return cudaGetLastError();
 }
 

@@ -5,6 +5,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -51,6 +52,8 @@ struct Context {
   std::string error;
   int64_t max_steps = 1 << 20;  // per-ray RKF step cap
   float z_window = 0.0f;        // adaptive render: z window of the block schedule (0 = none)
+  int32_t render_occupancy = 0; // adaptive render: blocks per SM (0 = register-limited)
+  int32_t render_engine = ILC_ENGINE_PERSISTENT;  // FP64 adaptive renders: kernel used
 
   // particle grid
   bool has_grid = false;
@@ -59,6 +62,8 @@ struct Context {
   DevBuf parts;      // float4 sorted particles
   DevBuf cells;      // int2 per grid cell
   DevBuf s2u;        // uint32 sorted -> original index
+  DevBuf codes;      // uint8 sub-box code per sorted particle (candidate pruning)
+  const uint32_t* sorted_keys = nullptr;  // cell key per sorted particle (keys_a or keys_b)
   DevBuf keys_a, keys_b, vals_a, vals_b, hist, tmp_in;  // build scratch
 
   // Gaunt table
@@ -80,6 +85,15 @@ struct Context {
 
   // adjoint: step checkpoints, per-cell derivatives, gradient accumulator
   DevBuf rec_h, rec_n, adj_dT, adj_dR, adj_grad, adj_seed, adj_loss;
+
+  // batched render: job table, sorted channel table, channel state, queue
+  DevBuf jobs, chan_sorted, chan_state, queue, item_cost, item_order;
+  int32_t batch_tile_w = 8;       // batched work item: tile_w x (32 / tile_w) pixels
+  int32_t batch_occupancy = 0;    // batched kernel: blocks per SM (0 = register-limited)
+  float batch_window = 0.0f;      // batched kernel: per-warp z window (0 = none)
+  bool batch_cost_order = true;   // hand out the costliest tiles first
+  cudaGraphExec_t batch_exec = nullptr;  // the batched launch sequence as a CUDA graph
+  std::string batch_key;                 // launch parameters it was captured with
 };
 
 // Error flags written by kernels (bit mask in flags[0]).
@@ -116,6 +130,9 @@ cudaError_t quantity_xray_flux_launch(Context& c, const float* rho, const float*
 cudaError_t quantity_xray_bin_launch(Context& c, const float* rho, const float* u,
                                      const float* xe, uint64_t n, float z, float dL, float e,
                                      float de, float* out);
+cudaError_t quantity_xray_bins_launch(Context& c, const float* rho, const float* u,
+                                      const float* xe, uint64_t n, float z, float dL,
+                                      const float* e, const float* de, int n_bins, float* out);
 cudaError_t quantity_temperature_launch(Context& c, const float* u, const float* xe,
                                         uint64_t n, float* out);
 
@@ -131,10 +148,13 @@ struct RenderArgs {
   bool apply_scale;
   float* out;           // device image
   float window_override = -1.0f;  // >= 0: z window for this launch (autotuner)
+  int occupancy_override = -1;    // >= 0: occupancy variant for this launch (autotuner)
   int row_stride = 1;             // > 1: only every row_stride-th tile row (autotuner)
   float* rec_h = nullptr;         // adjoint checkpoint: accepted step sizes per ray
   int32_t* rec_n = nullptr;
   int64_t rec_cap = 0;
+  const float* replay_h = nullptr;    // frozen replay: per-ray step sizes (rec_cap each)
+  const int32_t* replay_n = nullptr;  // frozen replay: steps per ray
 };
 
 // Adjoint of the X-ray band map (ilc_adjoint.cu).
@@ -148,11 +168,46 @@ cudaError_t adjoint_seed_launch(Context& c, const float* img, const float* targe
                                 float scale, float* seed, double* loss);
 // replay (checkpoint) or recompute the rays and scatter dL/dq (sorted order)
 cudaError_t adjoint_ray_launch(Context& c, const RenderArgs& a, int mode, const float* seed,
-                               float* grad, float* kernel_ms);
+                               double* grad, float* kernel_ms);
 // dL/dln rho, dL/dln T in the original order
-cudaError_t adjoint_chain_launch(Context& c, const float* grad, uint64_t n, const float* dq_lnrho,
+cudaError_t adjoint_chain_launch(Context& c, const double* grad, uint64_t n, const float* dq_lnrho,
                                  const float* dq_lnT, float* g_lnrho, float* g_lnT);
 cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms);
+
+// One camera of a batched render, as the kernel reads it.
+struct JobDev {
+  float look[3], b0[3], b1[3], minp[3];
+  float ps;
+  int32_t nx, ny, tiles_x;
+  double look_d[3], b0_d[3], b1_d[3], minp_d[3];
+  double ps_d;
+  double z_range, aperture, centre[3], radius, min_chord;
+  float scale;
+  int32_t pad;
+  uint64_t out_offset;
+  uint64_t item_begin;   // first work item (tile) of the job
+};
+
+struct BatchArgs {
+  const JobDev* jobs;     // device
+  int32_t n_jobs;
+  uint64_t n_items;
+  int32_t V;
+  const float* chan;      // device, sorted order, n x V (V = 1: nullptr = particles' q)
+  float* out;             // device images
+  double atol, rtol;
+  int32_t tile_w;         // 1, 2, 4, 8, 16 or 32
+  int32_t occupancy;      // 0, 3 or 4
+  float window;           // per-warp z window (0 = none)
+  const uint32_t* order;  // device: work item handed out q-th (nullptr = natural order)
+};
+// Estimated cost per work item of a batched render (the particles projected
+// into each tile's pixel columns, weighted by their cell's occupancy), and
+// the item order by decreasing cost.
+cudaError_t batched_order(Context& c, BatchArgs& a, const std::vector<JobDev>& jobs);
+// Sorted channel table: out[p * V + c] = in[s2u[p] * V + c].
+cudaError_t channels_sort_launch(Context& c, const float* in, uint64_t n, int V, float* out);
+cudaError_t batched_launch(Context& c, const BatchArgs& a, float* kernel_ms);
 
 // Spiral table (8 subcells x 125 offsets), generated on the host.
 void spiral_table(int8_t out[8][125][3]);

@@ -49,6 +49,27 @@ xray_bin_kernel(const float* __restrict__ table, GauntView G, const float* __res
   }
 }
 
+// xray_spectral_flux for n_bins bins at once (the quantity of each frame of
+// spectrum_generator, spectrum.cpp:89-109): out[b * n + i] for cell i, bin b.
+__global__ void __launch_bounds__(256)
+xray_bins_kernel(const float* __restrict__ table, GauntView G, const float* __restrict__ rho,
+                 const float* __restrict__ u, const float* __restrict__ xe, uint64_t n, float z,
+                 float dL, const float* __restrict__ e, const float* __restrict__ de, int n_bins,
+                 float* __restrict__ out) {
+  // cell-major output out[i * n_bins + b]: consecutive threads write
+  // consecutive bins of a cell, then the next cell
+  __shared__ float t[kMaxTable];
+  load_table(t, table, G.w * G.h);
+  const uint64_t total = n * (uint64_t)n_bins;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = k / (uint64_t)n_bins;
+    const int b = (int)(k - i * (uint64_t)n_bins);
+    const float T = temperature(u[i], xe[i]);
+    out[k] = brems(t, G, (1.f + z) * e[b], (1.f + z) * de[b], T, xe[i], rho[i], dL);
+  }
+}
+
 // mean_temperature (quantities.cl:268-284)
 __global__ void temperature_kernel(const float* __restrict__ u, const float* __restrict__ xe,
                                    uint64_t n, float* __restrict__ out) {
@@ -81,6 +102,16 @@ cudaError_t quantity_xray_bin_launch(Context& c, const float* rho, const float* 
   ++c.launches;
   xray_bin_kernel<<<persistent_blocks(n), 256, 0, c.stream>>>(c.gaunt.as<float>(), G, rho, u,
                                                               xe, n, z, dL, e, de, out);
+  return cudaGetLastError();
+}
+
+cudaError_t quantity_xray_bins_launch(Context& c, const float* rho, const float* u,
+                                      const float* xe, uint64_t n, float z, float dL,
+                                      const float* e, const float* de, int n_bins, float* out) {
+  GauntView G{c.gw, c.gh, c.gx0, c.gy0, c.gdx, c.gdy};
+  ++c.launches;
+  xray_bins_kernel<<<persistent_blocks(n * (uint64_t)n_bins), 256, 0, c.stream>>>(c.gaunt.as<float>(), G, rho, u, xe,
+                                                               n, z, dL, e, de, n_bins, out);
   return cudaGetLastError();
 }
 

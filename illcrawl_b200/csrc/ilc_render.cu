@@ -7,6 +7,9 @@
 // nn8 walk inline. A ray's state depends only on its own evaluations, so this
 // is the same computation as the reference's lock-step loop with stream
 // compaction, without its per-iteration host synchronisations.
+#include <cmath>
+#include <cstring>
+
 #include "ilc_device.cuh"
 #include "ilc_internal.h"
 #include "ilc_walk4.cuh"
@@ -15,6 +18,7 @@ namespace ilc {
 
 GridView make_grid_view(const Context& c) {
   GridView g;
+  std::memset(&g, 0, sizeof(g));  // padding too: the bytes key the batched launch graph
   g.min0 = c.gp.min[0]; g.min1 = c.gp.min[1]; g.min2 = c.gp.min[2];
   g.cs0 = c.gp.cs[0]; g.cs1 = c.gp.cs[1]; g.cs2 = c.gp.cs[2];
   g.half0 = 0.5f * c.gp.cs[0]; g.half1 = 0.5f * c.gp.cs[1]; g.half2 = 0.5f * c.gp.cs[2];
@@ -23,6 +27,11 @@ GridView make_grid_view(const Context& c) {
   g.n0 = c.gp.n[0]; g.n1 = c.gp.n[1]; g.n2 = c.gp.n[2];
   g.cells = c.cells.as<int2>();
   g.parts = c.parts.as<float4>();
+  g.codes = c.codes.as<uint32_t>();
+  g.inv_w0 = 4.0f / c.gp.cs[0];
+  g.inv_w1 = 4.0f / c.gp.cs[1];
+  g.inv_w2 = 4.0f / c.gp.cs[2];
+  g.margin = std::fmax(std::fmax(c.gp.cs[0], c.gp.cs[1]), c.gp.cs[2]) / 1024.0f;
   return g;
 }
 
@@ -35,6 +44,8 @@ struct RenderK {
   int controller;
   int64_t fixed_steps;
   float fixed_h;
+  const float* replay_h;    // frozen per-ray sequences (ray-major, rec_cap each)
+  const int32_t* replay_n;  // steps per ray
   int64_t max_steps;
   float window;     // z window of the adaptive schedule (<= 0: none)
   int row_stride;   // render every row_stride-th row of tiles (1 = all)
@@ -56,7 +67,8 @@ __device__ __forceinline__ void block_pixel(int row_stride, int& ix, int& iy) {
   iy = blockIdx.y * row_stride * kTileY + (warp >> 1) * 4 + (lane >> 3);
 }
 
-__global__ void __launch_bounds__(kRenderThreads)
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kRenderThreads, kMinBlocks)
 render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
               uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
   __shared__ char4 spiral[1000];
@@ -72,7 +84,28 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
   const float lx = a.cam.look0, ly = a.cam.look1, lz = a.cam.look2;
   float I = 0.0f, z = a.z0, h = 1.0f, k1 = 0.0f;
   float pts[4];
-  if (a.fixed_steps > 0) {
+  if (a.replay_h) {
+    if (active) {
+      // Frozen per-ray sequence: the given steps, every one accepted.
+      const int64_t ray = (int64_t)iy * a.cam.nx + ix;
+      const int64_t nr = a.replay_n[ray];
+      const int32_t n = (int32_t)(nr < 0 ? 0 : (nr > a.rec_cap ? a.rec_cap : nr));
+      const float* hs = a.replay_h + ray * a.rec_cap;
+      for (int32_t s = 0; s < n; ++s) {
+        h = hs[s];
+        rkf_points(z, h, pts);
+        float e[4];
+        nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
+        float d4 = 25.f / 216.f * k1 + 1408.f / 2565.f * e[0] + 2197.f / 4101.f * e[1] -
+                   1.f / 5.f * e[2];
+        d4 *= h;
+        I = I + d4;
+        z += h;
+        k1 = e[2];
+      }
+      steps = acc = (unsigned long long)(n > 0 ? n : 0);
+    }
+  } else if (a.fixed_steps > 0) {
     if (active) {
       // Frozen uniform sequence: every step accepted, I += delta4.
       h = a.fixed_h;
@@ -165,6 +198,8 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   k.controller = a.controller;
   k.fixed_steps = a.fixed_steps;
   k.fixed_h = a.fixed_h;
+  k.replay_h = a.replay_h;
+  k.replay_n = a.replay_n;
   k.max_steps = c.max_steps;
   k.window = a.window_override >= 0.0f ? a.window_override : c.z_window;
   k.row_stride = a.row_stride > 1 ? a.row_stride : 1;
@@ -182,9 +217,17 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   }
   cudaEventRecord(c.ev0, c.stream);
   ++c.launches;
-  render_kernel<<<grid, kRenderThreads, 0, c.stream>>>(
-      k, g, c.spiral.as<char4>(), c.flags.as<uint32_t>(),
-      reinterpret_cast<unsigned long long*>(c.flags.as<char>() + 64));
+  const int occ = a.occupancy_override >= 0 ? a.occupancy_override : c.render_occupancy;
+  unsigned long long* stats = reinterpret_cast<unsigned long long*>(c.flags.as<char>() + 64);
+  if (occ == 4)
+    render_kernel<4><<<grid, kRenderThreads, 0, c.stream>>>(k, g, c.spiral.as<char4>(),
+                                                            c.flags.as<uint32_t>(), stats);
+  else if (occ == 3)
+    render_kernel<3><<<grid, kRenderThreads, 0, c.stream>>>(k, g, c.spiral.as<char4>(),
+                                                            c.flags.as<uint32_t>(), stats);
+  else
+    render_kernel<1><<<grid, kRenderThreads, 0, c.stream>>>(k, g, c.spiral.as<char4>(),
+                                                            c.flags.as<uint32_t>(), stats);
   if ((e = cudaGetLastError())) return e;
   cudaEventRecord(c.ev1, c.stream);
   if (kernel_ms) {

@@ -22,6 +22,8 @@ struct Step4 {
   float qx[4], qy[4], qz[4];
   float d[4][8], v[4][8];
   float R[4], R2up[4];
+  float rr[4];    // (R + cell_radius)^2: the early-break threshold
+  float crad;     // cell radius
   int mi[4], cnt[4];
 };
 
@@ -36,6 +38,8 @@ template <int J> __device__ __forceinline__ void s4_rescan(Step4& s) {
   s.R[J] = r;
   s.mi[J] = m;
   s.R2up[J] = __fmul_ru(r, r);
+  const float b = r + s.crad;
+  s.rr[J] = b * b;
 }
 
 template <int J> __device__ __forceinline__ void s4_init(Step4& s) {
@@ -43,6 +47,8 @@ template <int J> __device__ __forceinline__ void s4_init(Step4& s) {
   for (int t = 0; t < 8; ++t) { s.d[J][t] = FLT_MAX; s.v[J][t] = 0.0f; }
   s.R[J] = FLT_MAX;
   s.R2up[J] = __int_as_float(0x7f800000);
+  const float b = FLT_MAX + s.crad;
+  s.rr[J] = b * b;
   s.mi[J] = 0;
   s.cnt[J] = 0;
 }
@@ -93,12 +99,90 @@ template <int J> __device__ __forceinline__ float s4_finalize(const Step4& s) {
   return res;
 }
 
+// Distance tests of one candidate against the active points.
+template <bool kSharedXY, bool kIdx>
+__device__ __forceinline__ void test_candidate(Step4& s, unsigned act, const float4& P, int p) {
+  float d2[4];
+  if (kSharedXY) {
+    const float fx = P.x - s.qx[0], fy = P.y - s.qy[0];
+    const float fxy = fx * fx + fy * fy;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float fz = P.z - s.qz[j];
+      d2[j] = fxy + fz * fz;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float fx = P.x - s.qx[j], fy = P.y - s.qy[j], fz = P.z - s.qz[j];
+      d2[j] = (fx * fx + fy * fy) + fz * fz;
+    }
+  }
+  const float pay = kIdx ? __int_as_float(p) : P.w;
+  s4_test<0>(s, act, d2[0], pay);
+  s4_test<1>(s, act, d2[1], pay);
+  s4_test<2>(s, act, d2[2], pay);
+  s4_test<3>(s, act, d2[3], pay);
+}
+
+// Cells with more candidates than this are scanned through their sub-box codes.
+constexpr int kPruneMin = 16;
+
+// Quarters [lo, hi] of one cell axis that the interval [a, b] touches, as a
+// 4-bit mask (0: none). t = (x - cell min) * 4 / cell size.
+__device__ __forceinline__ unsigned quarter_mask(float a, float b, float cmin, float inv_w) {
+  const float tl = (a - cmin) * inv_w, th = (b - cmin) * inv_w;
+  if (!(th >= 0.0f) || !(tl < 4.0f)) return 0u;
+  const int lo = tl > 0.0f ? (int)tl : 0;
+  const int hi = th < 4.0f ? (int)th : 3;
+  return (0xFu >> (3 - hi)) & (0xFu << lo);
+}
+
+// Bit (sx + 4 sy + 16 sz) set for every sub-box of the cell that meets the
+// box [qlo - ext, qhi + ext]: the union of the cubes of half-width
+// ext = max R + margin around the active points. A candidate in any other
+// sub-box is farther than its point's R from every active point (the margin
+// exceeds every rounding error of the codes and of the distance), so it
+// would not be inserted.
+__device__ __forceinline__ unsigned long long prune_mask(const GridView& g, int ix, int iy,
+                                                         int iz, const float qlo[3],
+                                                         const float qhi[3], float ext) {
+  const float mx = g.min0 + (float)ix * g.cs0;
+  const float my = g.min1 + (float)iy * g.cs1;
+  const float mz = g.min2 + (float)iz * g.cs2;
+  const unsigned xm = quarter_mask(qlo[0] - ext, qhi[0] + ext, mx, g.inv_w0);
+  const unsigned ym = quarter_mask(qlo[1] - ext, qhi[1] + ext, my, g.inv_w1);
+  const unsigned zm = quarter_mask(qlo[2] - ext, qhi[2] + ext, mz, g.inv_w2);
+  const unsigned ys = (ym & 1u) | ((ym & 2u) << 3) | ((ym & 4u) << 6) | ((ym & 8u) << 9);
+  const unsigned long long zs = (unsigned long long)(zm & 1u) |
+                                ((unsigned long long)(zm & 2u) << 15) |
+                                ((unsigned long long)(zm & 4u) << 30) |
+                                ((unsigned long long)(zm & 8u) << 45);
+  return (unsigned long long)(xm * ys) * zs;
+}
+
 // One walk over the spiral of (cx, cy, cz, sub) for the points in `mask`.
+// kSharedXY: all 4 points have bit-identical x and y (a view along the z
+// axis), so the x/y part of every squared distance, (dx*dx + dy*dy), is one
+// value for the 4 points and is evaluated once -- the same operations in the
+// same order, hence the same bits, as evaluating it per point.
+// kIdx: the slots carry the candidate's sorted index (as float bits) in
+// place of its value, for callers that look up several value channels.
+template <bool kSharedXY, bool kIdx>
 __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict__ spiral,
                                       Step4& s, unsigned mask, int cx, int cy, int cz, int sub,
                                       WalkStats& st) {
   const char4* order = spiral + sub * 125;
   unsigned act = mask;
+  // bounding box of the group's points (for the sub-box pruning)
+  float qlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, qhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if ((mask >> j) & 1u) {
+      qlo[0] = fminf(qlo[0], s.qx[j]); qhi[0] = fmaxf(qhi[0], s.qx[j]);
+      qlo[1] = fminf(qlo[1], s.qy[j]); qhi[1] = fmaxf(qhi[1], s.qy[j]);
+      qlo[2] = fminf(qlo[2], s.qz[j]); qhi[2] = fmaxf(qhi[2], s.qz[j]);
+    }
   for (int it = 0; it < 125; ++it) {
     const char4 o = order[it];
     const int ix = cx + o.x, iy = cy + o.y, iz = cz + o.z;
@@ -108,11 +192,20 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     {
       // early break per point: |c - q|^2 > (R + cell_radius)^2
       unsigned brk = 0;
+      if (kSharedXY) {
+        const float ex = ccx - s.qx[0], ey = ccy - s.qy[0];
+        const float exy = ex * ex + ey * ey;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float ex = ccx - s.qx[j], ey = ccy - s.qy[j], ez = ccz - s.qz[j];
-        const float r = s.R[j] + g.cell_radius;
-        if ((ex * ex + ey * ey) + ez * ez > r * r) brk |= 1u << j;
+        for (int j = 0; j < 4; ++j) {
+          const float ez = ccz - s.qz[j];
+          if (exy + ez * ez > s.rr[j]) brk |= 1u << j;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float ex = ccx - s.qx[j], ey = ccy - s.qy[j], ez = ccz - s.qz[j];
+          if ((ex * ex + ey * ey) + ez * ez > s.rr[j]) brk |= 1u << j;
+        }
       }
       act &= ~brk;
     }
@@ -126,18 +219,38 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     const unsigned na = __popc(act);
     st.cells += na;
     st.cands += na * (uint32_t)max(be.y - be.x, 0);
-    for (int p = be.x; p < be.y; ++p) {
-      const float4 P = __ldg(&g.parts[p]);
-      float d2[4];
+    if (be.x >= be.y) continue;
+    if (be.y - be.x > kPruneMin) {
+      float rmax = 0.0f;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float fx = P.x - s.qx[j], fy = P.y - s.qy[j], fz = P.z - s.qz[j];
-        d2[j] = (fx * fx + fy * fy) + fz * fz;
+      for (int j = 0; j < 4; ++j)
+        if ((act >> j) & 1u) rmax = fmaxf(rmax, s.R[j]);
+      const unsigned long long m = prune_mask(g, ix, iy, iz, qlo, qhi, rmax + g.margin);
+      if (m == 0ull) continue;
+      if (m != ~0ull) {
+        // candidates in ascending index order, 4 codes per word
+        for (int pw = be.x & ~3; pw < be.y; pw += 4) {
+          const uint32_t word = __ldg(&g.codes[pw >> 2]);
+          unsigned hits = 0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            hits |= (unsigned)((m >> ((word >> (8 * k)) & 63u)) & 1ull) << k;
+          if (pw < be.x) hits &= 0xFu << (be.x - pw);
+          if (be.y - pw < 4) hits &= 0xFu >> (4 - (be.y - pw));
+          while (hits) {
+            const int p = pw + __ffs(hits) - 1;
+            hits &= hits - 1;
+            test_candidate<kSharedXY, kIdx>(s, act, __ldg(&g.parts[p]), p);
+          }
+        }
+        continue;
       }
-      s4_test<0>(s, act, d2[0], P.w);
-      s4_test<1>(s, act, d2[1], P.w);
-      s4_test<2>(s, act, d2[2], P.w);
-      s4_test<3>(s, act, d2[3], P.w);
+    }
+    float4 P = __ldg(&g.parts[be.x]);
+    for (int p = be.x; p < be.y; ++p) {
+      const float4 N = (p + 1 < be.y) ? __ldg(&g.parts[p + 1]) : P;  // prefetch
+      test_candidate<kSharedXY, kIdx>(s, act, P, p);
+      P = N;
     }
   }
 }
@@ -160,12 +273,12 @@ __device__ __forceinline__ void locate(const GridView& g, float qx, float qy, fl
   sub = sx + 2 * sy + 4 * sz;
 }
 
-// nn8 values of the 4 points of one step (e[j] for point j).
-__device__ __forceinline__ void nn8_step4(const GridView& g, const char4* __restrict__ spiral,
-                                          float px, float py, float pz, float lx, float ly,
-                                          float lz, const float zq[4], float e[4],
-                                          WalkStats& st) {
-  Step4 s;
+// nn8 walk of the 4 points of one step; the slots are left in s.
+template <bool kIdx>
+__device__ __forceinline__ void nn8_walk_step4(const GridView& g,
+                                               const char4* __restrict__ spiral, float px,
+                                               float py, float pz, float lx, float ly, float lz,
+                                               const float zq[4], Step4& s, WalkStats& st) {
   int cx[4], cy[4], cz[4], sb[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -174,10 +287,19 @@ __device__ __forceinline__ void nn8_step4(const GridView& g, const char4* __rest
     s.qz[j] = pz + zq[j] * lz;
     locate(g, s.qx[j], s.qy[j], s.qz[j], cx[j], cy[j], cz[j], sb[j]);
   }
+  s.crad = g.cell_radius;
   s4_init<0>(s);
   s4_init<1>(s);
   s4_init<2>(s);
   s4_init<3>(s);
+  if (kIdx) {  // empty slots carry index -1
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int t = 0; t < 8; ++t) s.v[j][t] = __int_as_float(-1);
+  }
+  const bool shared_xy = s.qx[0] == s.qx[1] && s.qx[0] == s.qx[2] && s.qx[0] == s.qx[3] &&
+                         s.qy[0] == s.qy[1] && s.qy[0] == s.qy[2] && s.qy[0] == s.qy[3];
   unsigned todo = 0xFu;
   while (todo) {
     const int j0 = __ffs(todo) - 1;
@@ -190,9 +312,21 @@ __device__ __forceinline__ void nn8_step4(const GridView& g, const char4* __rest
     for (int j = 0; j < 4; ++j)
       if (((todo >> j) & 1u) && cx[j] == c0x && cy[j] == c0y && cz[j] == c0z && sb[j] == s0)
         mask |= 1u << j;
-    walk4(g, spiral, s, mask, c0x, c0y, c0z, s0, st);
+    if (shared_xy)
+      walk4<true, kIdx>(g, spiral, s, mask, c0x, c0y, c0z, s0, st);
+    else
+      walk4<false, kIdx>(g, spiral, s, mask, c0x, c0y, c0z, s0, st);
     todo &= ~mask;
   }
+}
+
+// nn8 values of the 4 points of one step (e[j] for point j).
+__device__ __forceinline__ void nn8_step4(const GridView& g, const char4* __restrict__ spiral,
+                                          float px, float py, float pz, float lx, float ly,
+                                          float lz, const float zq[4], float e[4],
+                                          WalkStats& st) {
+  Step4 s;
+  nn8_walk_step4<false>(g, spiral, px, py, pz, lx, ly, lz, zq, s, st);
   e[0] = s4_finalize<0>(s);
   e[1] = s4_finalize<1>(s);
   e[2] = s4_finalize<2>(s);

@@ -144,3 +144,35 @@ def scale_cells(n=67_108_864):
 def small_cells(n, seed=7, box=1000.0, r_s=100.0):
     """Small clustered set for parity tests (seconds on the oracle)."""
     return generate(n, box, [Halo((box / 2,) * 3, r_s, box / 2)], seed=seed)
+
+
+def gaussian_random_field_at(pos, box, sigma=0.1, ell=200.0, n=256, seed=20174):
+    """Seeded Gaussian random field on an n^3 periodic grid over [0, box]^3
+    (white noise filtered by exp(-k^2 ell^2 / 2) in Fourier space, then scaled
+    to standard deviation sigma), trilinearly interpolated at pos (N, 3).
+    The target perturbation of the adjoint workload: log T -> log T + field."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    white = rng.standard_normal((n, n, n))
+    k = 2.0 * np.pi * np.fft.fftfreq(n, d=box / n)
+    kz = 2.0 * np.pi * np.fft.rfftfreq(n, d=box / n)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2
+    f = np.fft.irfftn(np.fft.rfftn(white) * np.exp(-0.5 * k2 * ell * ell), s=(n, n, n))
+    f *= sigma / f.std()
+    g = np.asarray(pos, np.float64) / box * n - 0.5      # cell-centred samples
+    i0 = np.floor(g).astype(np.int64)
+    t = g - i0
+    out = np.zeros(len(g))
+    for dx in (0, 1):
+        wx = t[:, 0] if dx else 1.0 - t[:, 0]
+        for dy in (0, 1):
+            wy = t[:, 1] if dy else 1.0 - t[:, 1]
+            for dz in (0, 1):
+                wz = t[:, 2] if dz else 1.0 - t[:, 2]
+                idx = (i0 + np.array([dx, dy, dz])) % n
+                out += wx * wy * wz * f[idx[:, 0], idx[:, 1], idx[:, 2]]
+    return out
+
+
+def perturbed_internal_energy(cells, field):
+    """u for log T + field (T is proportional to u at fixed x_e)."""
+    return (cells.u.astype(np.float64) * np.exp(field)).astype(np.float32)

@@ -109,6 +109,21 @@ void* ilc_get_stream(ilc_ctx* ctx);
  * z_window-thick slabs together (0 = every ray runs to its end independently).
  * Changes the order of work only, never a result. */
 ilc_status ilc_set_z_window(ilc_ctx* ctx, float z_window);
+/* Kernel behind ilc_render_adaptive and ilc_project_xray_flux with the FP64
+ * controller. GRID: one thread block per 16 x 8 pixel tile, one launch per
+ * image (the reference's one-projection-per-call structure). PERSISTENT: the
+ * work-queue kernel of ilc_render_batched with this one camera (its
+ * schedule: ilc_set_batch_schedule). Both give the same image bit for bit;
+ * the REF32 controller, the fixed-step mode and the adjoint's forward pass
+ * always use GRID. Default: PERSISTENT. */
+enum { ILC_ENGINE_GRID = 0, ILC_ENGINE_PERSISTENT = 1 };
+ilc_status ilc_set_render_engine(ilc_ctx* ctx, int32_t engine);
+
+/* Occupancy of the adaptive render: 0 = as many blocks per SM as the
+ * kernel's registers allow, 3 or 4 = that many 128-thread blocks per SM
+ * (registers capped, some spilled). Changes the order of work only, never a
+ * result. */
+ilc_status ilc_set_render_occupancy(ilc_ctx* ctx, int32_t blocks_per_sm);
 
 /* ---- particle grid + nn8 backend ------------------------------------------
  * ilc_nn8_setup_particles replaces reconstruction_backend::setup_particles
@@ -167,6 +182,16 @@ ilc_status ilc_quantity_xray_spectral_flux(ilc_ctx* ctx, const float* rho, const
                                            float energy_bin_width, float* out,
                                            int is_device);
 
+/* Per-cell flux in n_bins energy bins at once, cell-major: out[i * n_bins + b]
+ * = xray_spectral_flux (quantities.cl:400-430) at energies[b], widths[b]; the
+ * per-bin values of xray_spectrum_quantity_generator (spectrum.cpp:89-109)
+ * in the layout ilc_render_batched reads. energies, widths: host arrays. */
+ilc_status ilc_quantity_xray_spectrum(ilc_ctx* ctx, const float* rho, const float* u,
+                                      const float* xe, uint64_t n, float redshift,
+                                      float luminosity_distance, const float* energies,
+                                      const float* widths, int32_t n_bins, float* out,
+                                      int is_device);
+
 /* Per-cell temperature [K]: mean_temperature (quantities.cl:268-284). */
 ilc_status ilc_quantity_temperature(ilc_ctx* ctx, const float* u, const float* xe, uint64_t n,
                                     float* out, int is_device);
@@ -196,6 +221,29 @@ ilc_status ilc_render_fixed(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
                             int64_t num_steps, const ilc_los_scaling* scaling, float* image,
                             int is_device, ilc_render_stats* stats);
 
+/* Adaptive render that also records every ray's accepted step sizes: ray
+ * k = iy * num_pix_x + ix writes n_steps[k] (at most capacity) sizes to
+ * step_sizes[k * capacity ...]. A ray with more accepted steps than capacity
+ * keeps its first capacity steps and the call returns ILC_ERR_INVALID_ARGUMENT
+ * after the render ("capacity too small"). The parity checkpoint of the
+ * frozen-sequence replay; no reference counterpart as an entry point.
+ * step_sizes / n_steps follow steps_on_device; image follows is_device. */
+ilc_status ilc_render_record(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                             ilc_tolerance tol, int32_t controller, float* step_sizes,
+                             int32_t* n_steps, int64_t capacity, int steps_on_device,
+                             float* image, int is_device, ilc_render_stats* stats);
+
+/* Frozen per-ray step sequence: ray k replays step_sizes[k * capacity + i],
+ * i < n_steps[k], every step accepted (I += delta4 of integration.cl:63-79,
+ * k1 carried), from z = 0. Replaying a recorded adaptive sequence gives the
+ * adaptive render's pixels; replaying it in double (the FP64 oracle) bounds
+ * the fp32 path's error at a fixed sequence. z_range is the nominal depth,
+ * used only by the scaling. No reference counterpart as an entry point. */
+ilc_status ilc_render_frozen(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                             const float* step_sizes, const int32_t* n_steps, int64_t capacity,
+                             int steps_on_device, const ilc_los_scaling* scaling, float* image,
+                             int is_device, ilc_render_stats* stats);
+
 /* The multiplier applied to every pixel by volumetric_integration.cpp:74-87. */
 float ilc_los_scale(const ilc_camera* cam, double z_range, const ilc_los_scaling* scaling);
 
@@ -212,6 +260,74 @@ ilc_status ilc_project_xray_flux(ilc_ctx* ctx, const float* cells, const float* 
                                  ilc_tolerance tol, int32_t controller,
                                  const ilc_los_scaling* scaling, float* image, int is_device,
                                  ilc_render_stats* stats);
+
+/* ---- batched render ---------------------------------------------------------
+ * Many projections in one persistent launch: the (camera, frame) loop of
+ * integrated_projection / distributed_animation (animation.cpp:29-100,229-241)
+ * and the per-bin loop of multi_quantity_integrated_projection /
+ * spectrum_generator (animation.cpp:264-283, spectrum.hpp:81-126) as one
+ * work queue of 32-ray tiles over all jobs, with V value channels per cell
+ * integrated along each ray together.
+ *
+ * A job is one camera. Its rays start on the camera plane like
+ * ilc_render_adaptive's and run along look_at over [0, z_range], or, when
+ * sphere_radius > 0, over the ray's chord of that sphere (widened about its
+ * midpoint to at least min_chord, clipped to start at the camera plane).
+ * aperture_radius > 0 masks pixels whose centre lies farther than that from
+ * the screen centre (their outputs are 0). Each ray's V channels are
+ * integrated with one step sequence from a joint FP64 controller: per channel
+ * the reference's error ratio (integration.cl:82-131 with the FP64
+ * controller), minimum over channels; a step is accepted only if every
+ * channel accepts it. With V = 1 and no mask or chord a job equals
+ * ilc_render_adaptive with ILC_CONTROLLER_FP64 bit for bit. For V > 1 the
+ * channels' step sequence differs from V separate renders (it is at least as
+ * fine as each channel's own).
+ *
+ * values: n x V floats, cell-major, in the order of the particles given to
+ * ilc_nn8_setup_particles (which must have been called; their q is not used).
+ * images: job k's V x num_pix_y x num_pix_x block (channel-major, row = y) at
+ * element out_offset, multiplied by scale. images_len bounds every block.
+ * V <= 256. stats may be NULL. */
+typedef struct ilc_job {
+  ilc_camera camera;
+  double z_range;          /* integration depth when sphere_radius <= 0 */
+  double aperture_radius;  /* <= 0: no mask */
+  double sphere_center[3];
+  double sphere_radius;    /* > 0: integrate over the chord of this sphere */
+  double min_chord;        /* chords shorter than this are widened to it */
+  float scale;             /* output multiplier, e.g. ilc_los_scale(...) */
+  int32_t reserved;        /* 0 */
+  uint64_t out_offset;     /* element offset of this job's block in images */
+} ilc_job;
+
+ilc_status ilc_render_batched(ilc_ctx* ctx, const float* values, int32_t n_channels,
+                              int values_on_device, const ilc_job* jobs, int32_t n_jobs,
+                              ilc_tolerance tol, float* images, uint64_t images_len,
+                              int images_on_device, ilc_render_stats* stats);
+
+/* Schedule of ilc_render_batched: work items are tiles of tile_w x
+ * (32 / tile_w) pixels (tile_w in 1, 2, 4, 8, 16, 32), one per warp; 0
+ * (register-limited), 3 or 4 blocks per SM; z_window > 0 makes a warp's rays
+ * advance in windows of that depth (they query one slab of the grid at a
+ * time); cost_order != 0 hands out the tiles in decreasing order of an
+ * estimated cost (particles projected into each tile's columns, weighted by
+ * their cell's occupancy), so the longest rays start first. Changes the order
+ * of work only, never a result. Default: 8, 0, 0, 1. */
+ilc_status ilc_set_batch_schedule(ilc_ctx* ctx, int32_t tile_w, int32_t blocks_per_sm,
+                                  float z_window, int32_t cost_order);
+
+/* Autotuner of the batched render's schedule: renders the jobs once per
+ * (tile_w, occupancy, z_window) candidate (outputs discarded, cost order on),
+ * times the kernel with CUDA events, sets the fastest and returns it
+ * (times_ms, may be NULL: n_tiles x n_occupancies x n_windows, in that
+ * nesting). Callers pass a representative subset of their jobs (e.g. the
+ * same cameras at a lower resolution). */
+ilc_status ilc_autotune_batched(ilc_ctx* ctx, const float* values, int32_t n_channels,
+                                int values_on_device, const ilc_job* jobs, int32_t n_jobs,
+                                ilc_tolerance tol, const int32_t* tile_ws, int32_t n_tiles,
+                                const int32_t* occupancies, int32_t n_occupancies,
+                                const float* windows, int32_t n_windows, int32_t* best_tile_w,
+                                int32_t* best_occupancy, float* best_window, float* times_ms);
 
 /* ---- adjoint ------------------------------------------------------------
  * Gradient of L = sum over pixels of (log I - log I_target)^2 for the X-ray
@@ -245,15 +361,16 @@ ilc_status ilc_adjoint_xray_flux(ilc_ctx* ctx, const float* cells, const float* 
                                  ilc_adjoint_stats* stats);
 
 /* Autotuner of the adaptive render's schedule: renders every sample_stride-th
- * row of 8-pixel tiles of the view once per candidate z window, times the
- * render kernel with CUDA events, sets the fastest on the context and returns
- * it in *best (times_ms, may be NULL: n_candidates kernel times). Needs the
- * particles set up. The result depends on the particle distribution and the
- * view, so callers cache it per workload. */
-ilc_status ilc_autotune_z_window(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
-                                 ilc_tolerance tol, int32_t controller, const float* candidates,
-                                 int32_t n_candidates, int32_t sample_stride, float* best,
-                                 float* times_ms);
+ * row of 8-pixel tiles of the view once per (z window, occupancy) candidate
+ * pair, times the render kernel with CUDA events, sets the fastest pair on the
+ * context and returns it (times_ms, may be NULL: n_windows x n_occupancies
+ * kernel times, window-major). Needs the particles set up. The result depends
+ * on the particle distribution and the view, so callers cache it per workload. */
+ilc_status ilc_autotune_render(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                               ilc_tolerance tol, int32_t controller, const float* windows,
+                               int32_t n_windows, const int32_t* occupancies,
+                               int32_t n_occupancies, int32_t sample_stride, float* best_window,
+                               int32_t* best_occupancy, float* times_ms);
 
 /* Allocation-free grid build, for callers that cannot allocate device memory
  * when they need a grid (for example while a CUDA graph is being captured, in

@@ -281,3 +281,71 @@ def adjoint(grid, cam, hs, n, gI, pix=None, precision=1, nthreads=0):
     _adj_lib().orc_adjoint(grid.h, ctypes.byref(cam), _p(pixa), hs.shape[0], _p(hs), hs.shape[1],
                            _p(n), _p(gI), precision, _p(grad), nthreads)
     return grad
+
+
+# ---- batched render (jobs = cameras with masks and chords, V channels) ----
+class OracleJob(ctypes.Structure):
+    _fields_ = [("camera", OracleCamera), ("z_range", ctypes.c_double),
+                ("aperture_radius", ctypes.c_double), ("sphere_center", ctypes.c_double * 3),
+                ("sphere_radius", ctypes.c_double), ("min_chord", ctypes.c_double),
+                ("scale", ctypes.c_float), ("pad", ctypes.c_int32),
+                ("out_offset", ctypes.c_uint64)]
+
+
+def _declare_batched(L):
+    P, i64 = ctypes.c_void_p, ctypes.c_int64
+    L.orc_render_batched.argtypes = [P, P, ctypes.c_int32, P, ctypes.c_int32, ctypes.c_double,
+                                     ctypes.c_double, i64, P, i64, ctypes.c_int, P, P,
+                                     ctypes.c_int]
+    L.orc_ray_span.argtypes = [P, ctypes.c_int32, ctypes.c_int32, P, P, P]
+
+
+def job(cam, z_range=0.0, aperture_radius=0.0, sphere_center=(0.0, 0.0, 0.0),
+        sphere_radius=0.0, min_chord=0.0, scale=1.0, out_offset=0):
+    return OracleJob(cam, z_range, aperture_radius, (ctypes.c_double * 3)(*sphere_center),
+                     sphere_radius, min_chord, scale, 0, out_offset)
+
+
+def jobs_array(jobs):
+    arr = (OracleJob * len(jobs))()
+    for i, j in enumerate(jobs):
+        arr[i] = j
+    return arr
+
+
+def render_batched(grid, values, jobs, atol=0.0, rtol=1e-3, rays=None, precision=0,
+                   max_steps=1 << 22, nthreads=0):
+    """values: (n,) or (n, V) per-cell channels in original order. rays: None
+    (whole images at the job offsets; returns the flat image buffer) or an
+    (m, 2) array of (job, pixel) pairs (returns m x V). Returns (out, stats4, rc)."""
+    L = lib()
+    if not hasattr(L, "_batched_declared"):
+        _declare_batched(L)
+        L._batched_declared = True
+    vals = np.ascontiguousarray(values, np.float32)
+    V = 1 if vals.ndim == 1 else vals.shape[1]
+    arr = jobs_array(jobs)
+    if rays is None:
+        total = max(int(j.out_offset) + V * j.camera.nx * j.camera.ny for j in jobs)
+        out = np.zeros(total, np.float32)
+        ra, nr = None, 0
+    else:
+        ra = np.ascontiguousarray(rays, np.int64).reshape(-1, 2)
+        nr = ra.shape[0]
+        out = np.zeros((nr, V), np.float32)
+    st = np.zeros(4, np.uint64)
+    rc = L.orc_render_batched(grid.h, _p(vals), V, ctypes.byref(arr), len(jobs), atol, rtol,
+                              max_steps, _p(ra), nr, precision, _p(out), _p(st), nthreads)
+    return out, st, rc
+
+
+def ray_span(jb, ix, iy):
+    L = lib()
+    if not hasattr(L, "_batched_declared"):
+        _declare_batched(L)
+        L._batched_declared = True
+    m = ctypes.c_int32(0)
+    o = np.zeros(3, np.float32)
+    ln = ctypes.c_float(0.0)
+    L.orc_ray_span(ctypes.byref(jb), ix, iy, ctypes.byref(m), _p(o), ctypes.byref(ln))
+    return bool(m.value), o, ln.value

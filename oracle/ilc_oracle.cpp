@@ -925,6 +925,196 @@ static void adjoint_ray(const Grid& g, const RayGeom<R>& rg, R z0, const float* 
 // ==========================================================================
 using namespace orc;
 
+// --------------------------------------------------------------------------
+// Batched render: many cameras (jobs), aperture masks, per-ray chords and V
+// value channels per cell in one pass. Not a reference function: it restates
+// the batched kernel's definition so the kernel can be checked bit for bit.
+// With V = 1, no mask and no chord it equals orc_render in the FP64
+// controller mode. The reference renders a spectrum as one projection per
+// energy bin (spectrum.cpp:89-109, animation.cpp:264-283); here the V
+// channels of a ray share one step sequence, driven by a joint FP64
+// controller: per channel the single-channel error ratio
+//   x_c = max(atol, |I_c/z' rtol|) h / (2 |d5_c - d4_c|)   (16 if d4_c == d5_c)
+// and s = (min_c x_c)^(1/4), which is the smallest of the per-channel step
+// factors (sqrt is monotone, so the min commutes with it exactly); a step
+// is accepted only when every channel would accept it.
+// --------------------------------------------------------------------------
+struct Job {
+  Camera cam;
+  double z_range;          // depth when no chord sphere is set
+  double aperture;         // > 0: pixel centres farther than this from the screen centre are masked
+  double centre[3];        // chord sphere
+  double radius;           // > 0: integrate over the ray's chord of the sphere
+  double min_chord;        // chords shorter than this are widened about their midpoint
+  float scale;             // output = I * scale
+  int32_t pad;
+  uint64_t offset;         // element offset of the job's V x ny x nx block
+};
+
+struct RaySpan { int masked; float origin[3]; float len; };
+
+// Mask, chord and float origin of one ray; every step is a plain IEEE
+// double or float operation (no contraction), as the kernel evaluates it.
+static void ray_span(const Job& j, const CamDev& d, int ix, int iy, RaySpan* r) {
+  r->masked = 0;
+  if (j.aperture > 0.0) {
+    const double dx = ((double)ix + 0.5 - 0.5 * (double)j.cam.nx) * d.ps_d;
+    const double dy = ((double)iy + 0.5 - 0.5 * (double)j.cam.ny) * d.ps_d;
+    if (dx * dx + dy * dy > j.aperture * j.aperture) r->masked = 1;
+  }
+  RayGeom<float> rg;
+  ray_geom_f(d, ix, iy, rg);
+  if (!(j.radius > 0.0)) {
+    for (int i = 0; i < 3; ++i) r->origin[i] = rg.pix[i];
+    r->len = (float)j.z_range;
+    return;
+  }
+  RayGeom<double> gd;
+  ray_geom_d(d, ix, iy, gd);
+  double w[3];
+  for (int i = 0; i < 3; ++i) w[i] = j.centre[i] - gd.pix[i];
+  const double t = (w[0] * d.look_d[0] + w[1] * d.look_d[1]) + w[2] * d.look_d[2];
+  const double ww = (w[0] * w[0] + w[1] * w[1]) + w[2] * w[2];
+  const double b2 = ww - t * t;
+  const double r2 = j.radius * j.radius;
+  double half = b2 < r2 ? std::sqrt(r2 - b2) : 0.0;
+  const double mh = 0.5 * j.min_chord;
+  if (half < mh) half = mh;
+  double z0 = t - half;
+  const double z1 = t + half;
+  if (z0 < 0.0) z0 = 0.0;
+  r->len = z1 > z0 ? (float)(z1 - z0) : 0.0f;
+  const float z0f = (float)z0;
+  for (int i = 0; i < 3; ++i) r->origin[i] = rg.pix[i] + z0f * d.look[i];
+}
+
+// Joint FP64 controller over V fp32 channels (see above); for V = 1 it is
+// rkf_advance_fp64 operation for operation.
+static void rkf_advance_multi(float* I, float& z, float& h, float* k1, int V, double atol,
+                              double rtol, float end, const float* e, float eps, float hmin,
+                              float hmax, float next[4], float* est) {
+  const double hd = (double)h;
+  const float znew = z + h;
+  double xmin = 0.0;
+  for (int c = 0; c < V; ++c) {
+    const double e0 = (double)e[c], e1 = (double)e[V + c], e2 = (double)e[2 * V + c],
+                 e3 = (double)e[3 * V + c];
+    double d4 = 25.0 / 216.0 * (double)k1[c] + 1408.0 / 2565.0 * e0 + 2197.0 / 4101.0 * e1 -
+                1.0 / 5.0 * e2;
+    double d5 = 16.0 / 135.0 * (double)k1[c] + 6656.0 / 12825.0 * e0 +
+                28561.0 / 56430.0 * e1 - 9.0 / 50.0 * e2 + 2.0 / 55.0 * e3;
+    d4 *= hd;
+    d5 *= hd;
+    est[c] = (float)((double)I[c] + d4);
+    double x = 16.0;
+    if (d4 != d5) {
+      const double err = std::fabs(d5 - d4);
+      const double srt = std::fabs((double)I[c] / (double)znew * rtol);
+      const double ot = std::fmax(atol, srt);
+      x = ot * hd / (2.0 * err);
+    }
+    if (c == 0 || x < xmin) xmin = x;
+  }
+  double s = std::sqrt(std::sqrt(xmin));
+  double nh = s * hd;
+  if (nh < (double)hmin) nh = (double)hmin;
+  else if (nh > (double)hmax) nh = (double)hmax;
+  s = nh / hd;
+  if (!(s < 0.95)) {
+    z = znew;
+    for (int c = 0; c < V; ++c) { I[c] = est[c]; k1[c] = e[2 * V + c]; }
+  }
+  h = (float)nh;
+  if (z + h >= end) h = end - z + eps;
+  rkf_points<float>(z, h, next);
+}
+
+// Channel values at one point: nn8 slots (sorted indices) applied to each
+// channel with nn8_finalize's operation order; empty slots carry value 0.
+template <class R>
+static void eval_channels(const Grid& g, const float* vs, int V, R x, R y, R z, R* out,
+                          SearchStats* st) {
+  Slots<R> s;
+  slots_init(s);
+  nn8_search<R>(g, x, y, z, s, st);
+  R w[8];
+  for (int j = 0; j < 8; ++j) w[j] = weight3d(s.d[j]);
+  R ws = (R)0;
+  for (int j = 0; j < 8; ++j) ws += w[j];
+  for (int c = 0; c < V; ++c) {
+    R dot = (R)0;
+    for (int j = 0; j < 8; ++j) {
+      const R v = s.id[j] >= 0 ? (R)vs[(size_t)s.id[j] * V + c] : (R)0;
+      dot = mathf<R>::fma(w[j], v, dot);
+    }
+    out[c] = (ws != (R)0 && dot != (R)0) ? dot / ws : (R)0;
+  }
+}
+
+static RayResult integrate_multi(const Grid& g, const float* vs, int V, const RaySpan& sp,
+                                 const float* look, double atol, double rtol,
+                                 int64_t max_steps, SearchStats* st, float* I) {
+  std::vector<float> k1(V, 0.0f), e(4 * (size_t)V), est(V);
+  for (int c = 0; c < V; ++c) I[c] = 0.0f;
+  float z = 0.0f, h = 1.0f;
+  float pts[4];
+  rkf_points<float>(0.0f, 1.0f, pts);
+  RayResult rr{0.f, 0, 0, 0};
+  while (z < sp.len) {
+    if (rr.steps >= max_steps) { rr.status = 1; break; }
+    for (int j = 0; j < 4; ++j)
+      eval_channels<float>(g, vs, V, sp.origin[0] + pts[j] * look[0],
+                           sp.origin[1] + pts[j] * look[1], sp.origin[2] + pts[j] * look[2],
+                           &e[(size_t)j * V], st);
+    const float zb = z;
+    rkf_advance_multi(I, z, h, k1.data(), V, atol, rtol, sp.len, e.data(), kEps, kHmin, kHmax,
+                      pts, est.data());
+    rr.steps += 1;
+    if (z != zb) rr.accepted += 1;
+  }
+  return rr;
+}
+
+// FP64 accuracy reference of one channel of a batched ray: the channel on
+// its own (its own step sequence, as the reference's per-bin projection),
+// everything in double from the double pixel position and chord.
+static float integrate_channel_d(const Grid& g, const float* vs, int V, int c, const Job& j,
+                                 const CamDev& d, int ix, int iy, double atol, double rtol,
+                                 int64_t max_steps, int* status) {
+  RayGeom<double> rg;
+  ray_geom_d(d, ix, iy, rg);
+  double z0 = 0.0, len = j.z_range;
+  if (j.radius > 0.0) {
+    double w[3];
+    for (int i = 0; i < 3; ++i) w[i] = j.centre[i] - rg.pix[i];
+    const double t = (w[0] * d.look_d[0] + w[1] * d.look_d[1]) + w[2] * d.look_d[2];
+    const double b2 = ((w[0] * w[0] + w[1] * w[1]) + w[2] * w[2]) - t * t;
+    double half = b2 < j.radius * j.radius ? std::sqrt(j.radius * j.radius - b2) : 0.0;
+    if (half < 0.5 * j.min_chord) half = 0.5 * j.min_chord;
+    z0 = t - half;
+    const double z1 = t + half;
+    if (z0 < 0.0) z0 = 0.0;
+    len = z1 > z0 ? z1 - z0 : 0.0;
+  }
+  double o[3];
+  for (int i = 0; i < 3; ++i) o[i] = rg.pix[i] + z0 * rg.look[i];
+  double I = 0., z = 0., h = 1.0, k1 = 0.0;
+  double pts[4] = {3. / 8., 12. / 13., 1.0, 0.5};
+  int64_t steps = 0;
+  *status = 0;
+  while (z < len) {
+    if (steps >= max_steps) { *status = 1; break; }
+    double e[4];
+    for (int q = 0; q < 4; ++q)
+      eval_channels<double>(g, vs + c, V, o[0] + pts[q] * rg.look[0], o[1] + pts[q] * rg.look[1],
+                            o[2] + pts[q] * rg.look[2], &e[q], nullptr);
+    rkf_advance_ref<double>(I, z, h, k1, atol, rtol, len, e, (double)kEps, (double)kHmin,
+                            (double)kHmax, pts);
+    ++steps;
+  }
+  return (float)I;
+}
+
 extern "C" {
 
 typedef struct {
@@ -1331,6 +1521,92 @@ int orc_xray_bin(const float* table, int w, int hgt, const float* rho, const flo
       out[i] = (float)brems<double>(G, (1. + z) * E, (1. + z) * dE, T, xe[i], rho[i], dL);
     }
   }
+  return 0;
+}
+
+
+// Batched render (see Job). values: n x V, cell-major, original cell order.
+// rays == nullptr: every pixel of every job into images at the job offsets
+// (channel-major V x ny x nx), masked pixels 0. Otherwise rays holds
+// (job, pixel) pairs and out receives nrays x V. precision 0: the batched
+// fp32 kernel's definition; 1: each channel on its own in double.
+// stats4: steps, accepted steps, cells visited, candidates.
+int orc_render_batched(void* h, const float* values, int32_t V, const void* jobs_v,
+                       int32_t n_jobs, double atol, double rtol, int64_t max_steps,
+                       const int64_t* rays, int64_t nrays, int precision, float* out,
+                       uint64_t* stats4, int nthreads) {
+  Grid* g = (Grid*)h;
+  const Job* jobs = (const Job*)jobs_v;
+  const int64_t n = (int64_t)g->s2u.size();
+  std::vector<float> vs((size_t)n * V);
+  for (int64_t p = 0; p < n; ++p)
+    for (int c = 0; c < V; ++c) vs[(size_t)p * V + c] = values[(size_t)g->s2u[p] * V + c];
+  std::vector<CamDev> cams(n_jobs);
+  for (int k = 0; k < n_jobs; ++k) camera_setup(jobs[k].cam, &cams[k]);
+  std::vector<int64_t> list;
+  if (!rays) {
+    for (int k = 0; k < n_jobs; ++k)
+      for (int64_t p = 0; p < (int64_t)jobs[k].cam.nx * jobs[k].cam.ny; ++p) {
+        list.push_back(k);
+        list.push_back(p);
+      }
+    rays = list.data();
+    nrays = (int64_t)list.size() / 2;
+  }
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  uint64_t st_steps = 0, st_acc = 0, st_cells = 0, st_cands = 0;
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : st_steps, st_acc, st_cells, st_cands, bad)
+  for (int64_t k = 0; k < nrays; ++k) {
+    const Job& j = jobs[rays[2 * k]];
+    const CamDev& d = cams[rays[2 * k]];
+    const int64_t p = rays[2 * k + 1];
+    const int ix = (int)(p % j.cam.nx), iy = (int)(p / j.cam.nx);
+    std::vector<float> I(V, 0.0f);
+    RaySpan sp;
+    ray_span(j, d, ix, iy, &sp);
+    if (!sp.masked) {
+      if (precision == 0) {
+        SearchStats st;
+        RayResult rr = integrate_multi(*g, vs.data(), V, sp, d.look, atol, rtol, max_steps, &st,
+                                       I.data());
+        bad += rr.status;
+        st_steps += rr.steps;
+        st_acc += rr.accepted;
+        st_cells += st.cells;
+        st_cands += st.candidates;
+      } else {
+        for (int c = 0; c < V; ++c) {
+          int status = 0;
+          I[c] = integrate_channel_d(*g, vs.data(), V, c, j, d, ix, iy, atol, rtol, max_steps,
+                                     &status);
+          bad += status;
+        }
+      }
+    }
+    for (int c = 0; c < V; ++c) {
+      const float v = sp.masked ? 0.0f : I[c] * j.scale;
+      if (list.empty())
+        out[(size_t)k * V + c] = v;
+      else
+        out[j.offset + (size_t)c * j.cam.nx * j.cam.ny + (size_t)p] = v;
+    }
+  }
+  if (stats4) { stats4[0] = st_steps; stats4[1] = st_acc; stats4[2] = st_cells; stats4[3] = st_cands; }
+  return bad ? 1 : 0;
+}
+
+// Ray span of one pixel of a job (mask, float origin, length) for tests.
+int orc_ray_span(const void* job_v, int32_t ix, int32_t iy, int32_t* masked, float* origin3,
+                 float* len) {
+  const Job& j = *(const Job*)job_v;
+  CamDev d;
+  camera_setup(j.cam, &d);
+  RaySpan sp;
+  ray_span(j, d, ix, iy, &sp);
+  *masked = sp.masked;
+  for (int i = 0; i < 3; ++i) origin3[i] = sp.origin[i];
+  *len = sp.len;
   return 0;
 }
 

@@ -40,13 +40,25 @@ def test_gpu_adjoint_matches_fp64_oracle(ctx, oracle_mod, gaunt_table, mode):
     assert st["loss"] == pytest.approx(loss, rel=1e-9)
     gI = 2.0 * (np.log(Id) - np.log(target.astype(np.float64))) / Id
     grad_q = oracle_mod.adjoint(g, oracle_mod.camera(*args), hs, nacc, gI, precision=1)
-    want_r, want_t = grad_q * dqR, grad_q * dqT
-    for got, want in ((gr, want_r), (gt, want_t)):
+    grad_q32 = oracle_mod.adjoint(g, oracle_mod.camera(*args), hs, nacc, gI, precision=0)
+    for dq, got in ((dqR, gr), (dqT, gt)):
         got = got.astype(np.float64)
+        # against the FP64 replay: fp32 evaluation points and weights move a
+        # few cells' gradients by up to ~1 % (the fp32 oracle shows the same
+        # deviation), the bulk stays within 1e-3
+        want = grad_q * dq
         err = np.linalg.norm(got - want) / np.linalg.norm(want)
         assert err < 1e-3, err
         big = np.abs(want) > 1e-2 * np.abs(want).max()
-        assert np.max(np.abs(got[big] - want[big]) / np.abs(want[big])) < 1e-3
+        rel = np.abs(got[big] - want[big]) / np.abs(want[big])
+        print("vs FP64: norm", err, "q0.99", np.quantile(rel, 0.99), "max", rel.max())
+        assert np.quantile(rel, 0.99) < 1e-3 and rel.max() < 3e-2
+        # against the fp32 oracle adjoint (same arithmetic, other summation order)
+        want32 = np.asarray(grad_q32, np.float64) * dq
+        big = np.abs(want32) > 1e-2 * np.abs(want32).max()
+        rel32 = np.abs(got[big] - want32[big]) / np.abs(want32[big])
+        print("vs fp32 oracle: max", rel32.max())
+        assert rel32.max() < 1e-4
     assert st["forward_ms"] > 0 and st["adjoint_ms"] > 0
 
 

@@ -1,0 +1,181 @@
+"""GPU parity of the batched render (ilc_render_batched) against the oracle's
+batched definition: many cameras with aperture masks and sphere chords, V
+value channels per cell, one persistent launch over a work queue.
+
+* V = 1 without mask or chord equals the plain adaptive render bit for bit;
+* every job, mask, chord and channel equals the oracle's batched render bit
+  for bit, with the same step and search statistics;
+* the schedule (tile shape, occupancy) changes nothing;
+* X-ray spectra: the per-cell bin table equals the oracle's per-bin
+  xray_spectral_flux, and the jointly stepped channels stay within 2x the
+  RKF tolerance of the FP64 per-bin oracle (each bin on its own, as the
+  reference renders a spectrum)."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import same_bits
+
+pytestmark = pytest.mark.gpu
+
+
+def _cells(seed, n):
+    from illcrawl_b200 import synthetic
+    return synthetic.small_cells(n, seed=seed)
+
+
+def _dirs(rng, k):
+    v = rng.normal(size=(k, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _jobs(mod, rng, sizes, centre=(500.0, 500.0, 500.0), radius=420.0):
+    """Cameras around the halo: random directions and rolls, apertures and
+    chords of a sphere, built with either module's job() helper."""
+    jobs = []
+    for k, (nx, ny) in enumerate(sizes):
+        look = _dirs(rng, 1)[0]
+        pos = np.asarray(centre) - 600.0 * look
+        cam = mod.camera(tuple(pos), tuple(look), float(rng.uniform(0, 2 * np.pi)), 900.0, nx, ny)
+        kind = k % 3
+        if kind == 0:    # plain depth
+            jobs.append(mod.job(cam, z_range=1200.0, scale=1.5))
+        elif kind == 1:  # aperture + chord
+            jobs.append(mod.job(cam, aperture_radius=float(rng.uniform(150, 450)),
+                                sphere_center=centre, sphere_radius=radius, min_chord=84.0,
+                                scale=0.25))
+        else:            # chord only
+            jobs.append(mod.job(cam, sphere_center=centre, sphere_radius=radius,
+                                min_chord=84.0))
+    return jobs
+
+
+def _oracle_images(oracle_mod, g, vals, ojobs, V):
+    off = 0
+    for j in ojobs:
+        j.out_offset = off
+        off += V * j.camera.nx * j.camera.ny
+    out, st, rc = oracle_mod.render_batched(g, vals, ojobs, 0.0, 1e-3)
+    assert rc == 0
+    return out, st
+
+
+def test_batched_single_channel_equals_plain_render(ctx, oracle_mod):
+    import illcrawl_b200 as ilc
+    c = _cells(31, 30_000)
+    pts = c.xyzq(c.rho)
+    ctx.setup_particles(pts)
+    args = ((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 21, 13)
+    ctx.set_render_engine(ilc.ENGINE_GRID)
+    try:
+        img, st = ctx.render_adaptive(ilc.camera(*args), 1000.0, 1e-3, 0.0, 1)
+    finally:
+        ctx.set_render_engine(ilc.ENGINE_PERSISTENT)
+    out, bst = ctx.render_batched(c.rho, [ilc.job(ilc.camera(*args), z_range=1000.0)])
+    assert same_bits(out, img.ravel())
+    for k in ("steps", "accepted_steps", "cells_visited", "candidates"):
+        assert bst[k] == st[k], k
+
+
+@pytest.mark.parametrize("V", [1, 3, 37])
+def test_batched_jobs_bit_exact(ctx, oracle_mod, V):
+    import illcrawl_b200 as ilc
+    c = _cells(32, 25_000)
+    pts = c.xyzq(c.rho)
+    ctx.setup_particles(pts)
+    g = oracle_mod.Grid(pts)
+    rng = np.random.default_rng(5 + V)
+    vals = (c.rho[:, None] * rng.uniform(0.5, 2.0, size=(1, V))).astype(np.float32)
+    if V == 1:
+        vals = vals[:, 0].copy()
+    sizes = [(16, 12), (9, 20), (24, 8), (13, 13)]
+    jobs = _jobs(ilc, np.random.default_rng(77), sizes)
+    ojobs = _jobs(oracle_mod, np.random.default_rng(77), sizes)
+    out, st = ctx.render_batched(vals, jobs)
+    want, ost = _oracle_images(oracle_mod, g, vals, ojobs, V)
+    assert same_bits(out, want)
+    assert st["steps"] == ost[0] and st["accepted_steps"] == ost[1]
+    assert st["cells_visited"] == ost[2] and st["candidates"] == ost[3]
+    # masked pixels are 0 in every channel, and some are masked
+    assert np.sum(want == 0.0) > 0
+
+
+def test_batched_schedule_is_result_neutral(ctx):
+    import illcrawl_b200 as ilc
+    c = _cells(33, 20_000)
+    ctx.setup_particles(c.xyzq(c.rho))
+    vals = np.stack([c.rho, c.rho * 0.5, c.rho * c.rho], 1).astype(np.float32)
+    sizes = [(19, 11), (8, 8), (33, 5)]
+    ref = None
+    try:
+        for tw, occ, win, order in ((8, 0, 0.0, False), (1, 0, 0.0, True), (4, 3, 25.0, True),
+                                    (8, 4, 7.0, True), (32, 0, 60.0, False), (16, 3, 0.0, True)):
+            ctx.set_batch_schedule(tw, occ, win, order)
+            out, _ = ctx.render_batched(vals, _jobs(ilc, np.random.default_rng(3), sizes))
+            if ref is None:
+                ref = out.copy()
+            else:
+                assert same_bits(out, ref), (tw, occ, win, order)
+    finally:
+        ctx.set_batch_schedule()
+
+
+def test_batched_autotuner(ctx):
+    import illcrawl_b200 as ilc
+    c = _cells(34, 20_000)
+    ctx.setup_particles(c.xyzq(c.rho))
+    jobs = _jobs(ilc, np.random.default_rng(4), [(16, 16), (12, 20)])
+    try:
+        bt, bo, bw, times = ctx.autotune_batched(c.rho, jobs, tile_ws=(4, 32), occupancies=(0, 3),
+                                                 windows=(0.0, 20.0))
+        assert bt in (4, 32) and bo in (0, 3) and bw in (0.0, 20.0)
+        assert times[(bt, bo, bw)] == min(times.values()) and len(times) == 8
+    finally:
+        ctx.set_batch_schedule()
+
+
+def test_batched_rejects_bad_jobs(ctx):
+    import illcrawl_b200 as ilc
+    c = _cells(35, 5_000)
+    ctx.setup_particles(c.xyzq(c.rho))
+    cam = ilc.camera((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 8, 8)
+    with pytest.raises(ilc.IlcError):          # no depth and no chord
+        ctx.render_batched(c.rho, [ilc.job(cam)])
+    with pytest.raises(ilc.IlcError):          # V > 256
+        ctx.render_batched(np.zeros((c.n, 257), np.float32), [ilc.job(cam, z_range=10.0)])
+
+
+def test_spectrum_table_and_accuracy_vs_fp64(ctx, oracle_mod, gaunt_table):
+    """Per-cell bin table bit-exact; jointly stepped spectra within 2x the RKF
+    tolerance of the FP64 oracle rendering each bin on its own."""
+    import illcrawl_b200 as ilc
+    c = _cells(36, 30_000)
+    ctx.load_gaunt()
+    nb = 8
+    edges = np.geomspace(0.3, 10.0, nb + 1)
+    e = edges[:-1].astype(np.float32)
+    w = np.diff(edges).astype(np.float32)
+    tab = ctx.xray_spectrum(c.rho, c.u, c.xe, e, w)
+    for b in range(nb):
+        ob = oracle_mod.xray_bin(gaunt_table, c.rho, c.u, c.xe, 0.2, 978500.0, float(e[b]),
+                                 float(w[b]))
+        assert np.array_equal(tab[:, b].view(np.uint32), ob.view(np.uint32))
+    pts = c.xyzq(np.zeros(c.n, np.float32))
+    ctx.setup_particles(pts)
+    g = oracle_mod.Grid(pts)
+    sizes = [(12, 12), (10, 14)]
+    jobs = _jobs(ilc, np.random.default_rng(8), sizes)
+    ojobs = _jobs(oracle_mod, np.random.default_rng(8), sizes)
+    out, st = ctx.render_batched(tab, jobs)
+    want, _ = _oracle_images(oracle_mod, g, tab, ojobs, nb)
+    assert same_bits(out, want)
+    # FP64 per-bin oracle on a sample of rays of job 1 (masked pixels excluded)
+    rays = [(1, p) for p in range(0, sizes[1][0] * sizes[1][1], 7)]
+    ref, _, rc = oracle_mod.render_batched(g, tab, ojobs, 0.0, 1e-3, rays=rays, precision=1)
+    assert rc == 0
+    npix = sizes[1][0] * sizes[1][1]
+    off1 = nb * sizes[0][0] * sizes[0][1]
+    got = np.stack([out[off1 + b * npix + np.array([p for _, p in rays])] for b in range(nb)], 1)
+    ok = ref > 0
+    rel = np.abs(got[ok] - ref[ok]) / ref[ok]
+    print("spectrum vs FP64 per-bin: median", np.median(rel), "max", rel.max())
+    assert np.median(rel) < 2e-3 and np.quantile(rel, 0.9) < 2e-3 and rel.max() < 1e-2

@@ -149,15 +149,19 @@ def test_quantities_bit_exact(ctx, oracle_mod, gaunt_table):
     assert np.quantile(rel, 0.999) < 1e-4 and rel.max() < 1e-2
 
 
-@pytest.mark.parametrize("controller", [0, 1])
-def test_render_adaptive_bit_exact(ctx, oracle_mod, controller):
+@pytest.mark.parametrize("controller,engine", [(0, 0), (1, 0), (1, 1)])
+def test_render_adaptive_bit_exact(ctx, oracle_mod, controller, engine):
     c = _cells(21, 40_000)
     pts = c.xyzq(c.rho)
     ctx.setup_particles(pts)
     g = oracle_mod.Grid(pts)
     args = ((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 24, 20)
     import illcrawl_b200 as ilc
-    img, st = ctx.render_adaptive(ilc.camera(*args), 1000.0, 1e-3, 0.0, controller)
+    ctx.set_render_engine(engine)
+    try:
+        img, st = ctx.render_adaptive(ilc.camera(*args), 1000.0, 1e-3, 0.0, controller)
+    finally:
+        ctx.set_render_engine(ilc.ENGINE_PERSISTENT)
     out, steps, acc, ost, rc = g.render(oracle_mod.camera(*args), 1000.0, 0.0, 1e-3,
                                         mode=controller)
     assert rc == 0
@@ -175,10 +179,12 @@ def test_render_z_window_schedule_is_result_neutral(ctx, oracle_mod, window):
     g = oracle_mod.Grid(pts)
     args = ((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 33, 19)   # ragged vs the 16 x 8 tiles
     ctx.set_z_window(window)
+    ctx.set_render_engine(ilc.ENGINE_GRID)
     try:
         img, st = ctx.render_adaptive(ilc.camera(*args), 1000.0, 1e-3, 0.0, 1)
     finally:
         ctx.set_z_window(0.0)
+        ctx.set_render_engine(ilc.ENGINE_PERSISTENT)
     out, *_ = g.render(oracle_mod.camera(*args), 1000.0, 0.0, 1e-3, mode=1)
     assert np.array_equal(img.ravel().view(np.uint32), out.view(np.uint32))
 
@@ -189,14 +195,15 @@ def test_autotuner_picks_a_candidate_and_keeps_results(ctx, oracle_mod):
     pts = c.xyzq(c.rho)
     ctx.setup_particles(pts)
     args = ((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 64, 64)
-    best, times = ctx.autotune_z_window(ilc.camera(*args), 1000.0, 1e-3, candidates=(0, 8, 32),
-                                        sample_stride=2)
+    bw, bo, times = ctx.autotune_render(ilc.camera(*args), 1000.0, 1e-3, windows=(0, 8, 32),
+                                        occupancies=(0, 3, 4), sample_stride=2)
     try:
-        assert best in (0.0, 8.0, 32.0) and all(t > 0 for t in times.values())
-        assert times[best] == min(times.values())
+        assert bw in (0.0, 8.0, 32.0) and bo in (0, 3, 4) and all(t > 0 for t in times.values())
+        assert times[(bw, bo)] == min(times.values())
         img, _ = ctx.render_adaptive(ilc.camera(*args), 1000.0, 1e-3, 0.0, 1)
     finally:
         ctx.set_z_window(0.0)
+        ctx.set_render_occupancy(0)
     out, *_ = oracle_mod.Grid(pts).render(oracle_mod.camera(*args), 1000.0, 0.0, 1e-3, mode=1,
                                           pix=np.arange(0, 64 * 64, 97))
     assert np.array_equal(img.ravel()[::97].view(np.uint32), out.view(np.uint32))
@@ -261,3 +268,44 @@ def test_density_workload_sampled_pixels(ctx, oracle_mod):
     o64, *_ = g.render(oracle_mod.camera(*args), 3000.0, 0.0, 1e-3, mode=2, pix=pix)
     rel = np.abs(img.ravel()[pix] - o64) / np.abs(o64)
     assert np.median(rel) < 2e-3
+
+
+def test_render_record_and_frozen_replay(ctx, oracle_mod):
+    """Recorded adaptive sequences equal the oracle's; replaying them gives the
+    adaptive pixels bit for bit and stays within 1e-5 of the FP64 replay."""
+    import illcrawl_b200 as ilc
+    c = _cells(23, 30_000)
+    pts = c.xyzq(c.rho)
+    ctx.setup_particles(pts)
+    g = oracle_mod.Grid(pts)
+    args = ((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 12, 10)
+    cap = 8000
+    img, hs, n, st = ctx.render_record(ilc.camera(*args), 1000.0, cap)
+    oimg, ohs, on, orc = g.render_record(oracle_mod.camera(*args), 1000.0, 0.0, 1e-3, mode=1,
+                                         cap=cap)
+    assert orc == 0
+    assert np.array_equal(n, on)
+    for k in range(len(n)):
+        assert np.array_equal(hs[k, :n[k]].view(np.uint32), ohs[k, :n[k]].view(np.uint32))
+    assert same_bits(img.ravel(), oimg)
+    frozen, fst = ctx.render_frozen(ilc.camera(*args), 1000.0, hs, n)
+    assert same_bits(frozen.ravel(), img.ravel())
+    assert fst["steps"] == int(n.sum())
+    o64 = g.render_replay(oracle_mod.camera(*args), ohs, on, precision=1)
+    o64 = o64[1] if isinstance(o64, tuple) else o64
+    o64 = np.asarray(o64, np.float64)
+    ok = o64 != 0
+    rel = np.abs(frozen.ravel()[ok] - o64[ok]) / np.abs(o64[ok])
+    print("frozen fp32 vs FP64 replay: max rel", rel.max())
+    assert rel.max() < 1e-5
+
+
+def test_render_frozen_rejects_counts_beyond_capacity(ctx):
+    import illcrawl_b200 as ilc
+    c = _cells(24, 5_000)
+    ctx.setup_particles(c.xyzq(c.rho))
+    cam = ilc.camera((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 4, 4)
+    hs = np.full((16, 8), 1.0, np.float32)
+    n = np.full(16, 9, np.int32)
+    with pytest.raises(ilc.IlcError):
+        ctx.render_frozen(cam, 1000.0, hs, n)
