@@ -420,7 +420,7 @@ def run_ours(args, rank, world, local_rank):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        e2e_steps = max(1, min(args.steps, 2))
+        e2e_steps = 1
         e2e_s = 0.0
         for _ in range(e2e_steps):
             flush.fill_(2.0)
@@ -488,9 +488,9 @@ def main():
                     help="render kernel: persistent work queue (default) or one block per tile")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-plain spectral leg")
-    ap.add_argument("--batched-div", type=int, default=4,
+    ap.add_argument("--batched-div", type=int, default=8,
                     help="camera sides of the batched leg divided by this (bounded sample)")
-    ap.add_argument("--plain-bins", type=int, default=4,
+    ap.add_argument("--plain-bins", type=int, default=2,
                     help="bins timed in the plain per-(camera, bin) arm, scaled to 128")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
     ap.add_argument("--autotune", action="store_true",
