@@ -85,7 +85,8 @@ struct GridView {
   const int2* __restrict__ cells;     // [begin, end) per cell
   const float4* __restrict__ parts;   // (x, y, z, q) in cell order
   // Sub-box codes for exact candidate pruning: per sorted particle one byte,
-  // sx + 4 sy + 16 sz, its quarter of the cell per axis (4 per word).
+  // sx + 4 sy + 16 sz, its quarter of the cell per axis (read 16 at a time
+  // from a 16-byte aligned buffer padded to a multiple of 16 bytes).
   const uint32_t* __restrict__ codes;
   float inv_w0, inv_w1, inv_w2;       // 4 / cell size
   float margin;                       // slack covering float rounding (cell size / 1024)

@@ -283,7 +283,7 @@ cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n) {
   if ((e = c.keys_a.ensure(n * 4)) || (e = c.keys_b.ensure(n * 4)) ||
       (e = c.vals_a.ensure(n * 4)) || (e = c.vals_b.ensure(n * 4)) ||
       (e = c.parts.ensure(n * 16)) || (e = c.s2u.ensure(n * 4)) ||
-      (e = c.codes.ensure(((n + 3) / 4) * 4 + 16)) || (e = c.cells.ensure(g.total * 8)) ||
+      (e = c.codes.ensure(((n + 15) / 16) * 16 + 16)) || (e = c.cells.ensure(g.total * 8)) ||
       (e = c.flags.ensure(kFlagsBytes)))
     return e;
   const uint64_t tiles = (n + kSortTile - 1) / kSortTile;

@@ -221,30 +221,40 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     st.cands += na * (uint32_t)max(be.y - be.x, 0);
     if (be.x >= be.y) continue;
     if (be.y - be.x > kPruneMin) {
-      float rmax = 0.0f;
+      // Dense cell: candidates in ascending index order, 16 codes per chunk.
+      // The sub-box mask follows the search radius as it shrinks while the
+      // cell is scanned (a mask from a larger radius stays conservative), and
+      // once no sub-box is within reach no later candidate of the cell can be
+      // inserted.
+      float rused = -1.0f;
+      unsigned long long m = ~0ull;
+      for (int pw = be.x & ~15; pw < be.y; pw += 16) {
+        float rmax = 0.0f;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if ((act >> j) & 1u) rmax = fmaxf(rmax, s.R[j]);
-      const unsigned long long m = prune_mask(g, ix, iy, iz, qlo, qhi, rmax + g.margin);
-      if (m == 0ull) continue;
-      if (m != ~0ull) {
-        // candidates in ascending index order, 4 codes per word
-        for (int pw = be.x & ~3; pw < be.y; pw += 4) {
-          const uint32_t word = __ldg(&g.codes[pw >> 2]);
-          unsigned hits = 0;
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
-            hits |= (unsigned)((m >> ((word >> (8 * k)) & 63u)) & 1ull) << k;
-          if (pw < be.x) hits &= 0xFu << (be.x - pw);
-          if (be.y - pw < 4) hits &= 0xFu >> (4 - (be.y - pw));
-          while (hits) {
-            const int p = pw + __ffs(hits) - 1;
-            hits &= hits - 1;
-            test_candidate<kSharedXY, kIdx>(s, act, __ldg(&g.parts[p]), p);
-          }
+        for (int j = 0; j < 4; ++j)
+          if ((act >> j) & 1u) rmax = fmaxf(rmax, s.R[j]);
+        if (rmax != rused) {
+          m = prune_mask(g, ix, iy, iz, qlo, qhi, rmax + g.margin);
+          rused = rmax;
+          if (m == 0ull) break;
         }
-        continue;
+        const uint4 w4 = __ldg(reinterpret_cast<const uint4*>(g.codes) + (pw >> 4));
+        const uint32_t words[4] = {w4.x, w4.y, w4.z, w4.w};
+        unsigned hits = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            hits |= (unsigned)((m >> ((words[k] >> (8 * q)) & 63u)) & 1ull) << (4 * k + q);
+        if (pw < be.x) hits &= 0xFFFFu << (be.x - pw);
+        if (be.y - pw < 16) hits &= 0xFFFFu >> (16 - (be.y - pw));
+        while (hits) {
+          const int p = pw + __ffs(hits) - 1;
+          hits &= hits - 1;
+          test_candidate<kSharedXY, kIdx>(s, act, __ldg(&g.parts[p]), p);
+        }
       }
+      continue;
     }
     float4 P = __ldg(&g.parts[be.x]);
     for (int p = be.x; p < be.y; ++p) {

@@ -270,9 +270,12 @@ def test_density_workload_sampled_pixels(ctx, oracle_mod):
     assert np.median(rel) < 2e-3
 
 
-def test_render_record_and_frozen_replay(ctx, oracle_mod):
-    """Recorded adaptive sequences equal the oracle's; replaying them gives the
-    adaptive pixels bit for bit and stays within 1e-5 of the FP64 replay."""
+@pytest.mark.parametrize("controller", [0, 1])
+def test_render_record_and_frozen_replay(ctx, oracle_mod, controller):
+    """Recorded adaptive sequences equal the oracle's; replaying them equals the
+    oracle's replay bit for bit (and, with the fp32 controller whose steps add
+    fp32 increments like the replay, the adaptive pixels themselves), and stays
+    within 1e-5 of the FP64 replay."""
     import illcrawl_b200 as ilc
     c = _cells(23, 30_000)
     pts = c.xyzq(c.rho)
@@ -280,20 +283,22 @@ def test_render_record_and_frozen_replay(ctx, oracle_mod):
     g = oracle_mod.Grid(pts)
     args = ((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 12, 10)
     cap = 8000
-    img, hs, n, st = ctx.render_record(ilc.camera(*args), 1000.0, cap)
-    oimg, ohs, on, orc = g.render_record(oracle_mod.camera(*args), 1000.0, 0.0, 1e-3, mode=1,
-                                         cap=cap)
+    img, hs, n, st = ctx.render_record(ilc.camera(*args), 1000.0, cap, controller=controller)
+    oimg, ohs, on, orc = g.render_record(oracle_mod.camera(*args), 1000.0, 0.0, 1e-3,
+                                         mode=controller, cap=cap)
     assert orc == 0
     assert np.array_equal(n, on)
     for k in range(len(n)):
         assert np.array_equal(hs[k, :n[k]].view(np.uint32), ohs[k, :n[k]].view(np.uint32))
     assert same_bits(img.ravel(), oimg)
     frozen, fst = ctx.render_frozen(ilc.camera(*args), 1000.0, hs, n)
-    assert same_bits(frozen.ravel(), img.ravel())
+    assert same_bits(frozen.ravel(), g.render_replay(oracle_mod.camera(*args), ohs, on))
+    if controller == 0:
+        assert same_bits(frozen.ravel(), img.ravel())
+    else:  # the FP64 controller adds its increments in double
+        assert np.max(np.abs(frozen.ravel() - img.ravel()) / np.abs(img.ravel())) < 1e-6
     assert fst["steps"] == int(n.sum())
-    o64 = g.render_replay(oracle_mod.camera(*args), ohs, on, precision=1)
-    o64 = o64[1] if isinstance(o64, tuple) else o64
-    o64 = np.asarray(o64, np.float64)
+    o64 = np.asarray(g.render_replay(oracle_mod.camera(*args), ohs, on, precision=1), np.float64)
     ok = o64 != 0
     rel = np.abs(frozen.ravel()[ok] - o64[ok]) / np.abs(o64[ok])
     print("frozen fp32 vs FP64 replay: max rel", rel.max())
