@@ -150,6 +150,28 @@ __device__ __forceinline__ void store_slots(const Step4& s, RaySlots& r) {
   r.ws[J] = ws;
 }
 
+// One channel's FP64 step candidate: returns I + delta4 (as the accepted
+// value) and sets x to the channel's error ratio
+// max(atol, |I/z' rtol|) h / (2 |delta5 - delta4|), or 16 if delta4 == delta5.
+__device__ __forceinline__ float channel_step(float Ic, float k1c, float e0, float e1, float e2,
+                                              float e3, double hd, float znew, double atol,
+                                              double rtol, double& x) {
+  double d4 = 25.0 / 216.0 * (double)k1c + 1408.0 / 2565.0 * (double)e0 +
+              2197.0 / 4101.0 * (double)e1 - 1.0 / 5.0 * (double)e2;
+  double d5 = 16.0 / 135.0 * (double)k1c + 6656.0 / 12825.0 * (double)e0 +
+              28561.0 / 56430.0 * (double)e1 - 9.0 / 50.0 * (double)e2 + 2.0 / 55.0 * (double)e3;
+  d4 *= hd;
+  d5 *= hd;
+  x = 16.0;
+  if (d4 != d5) {
+    const double err = fabs(d5 - d4);
+    const double srt = fabs((double)Ic / (double)znew * rtol);
+    const double ot = fmax(atol, srt);
+    x = ot * hd / (2.0 * err);
+  }
+  return (float)((double)Ic + d4);
+}
+
 template <bool kMulti, int kMinBlocks>
 __global__ void __launch_bounds__(kBThreads, kMinBlocks)
 batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
@@ -243,40 +265,67 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
           // and are committed once the warp knows the step is accepted
           float* Es = Ks + a.V;
           float* E2s = Es + a.V;
+          if ((a.V & 3) == 0) {
+            // rows of V = 4G floats: lane handles float4 groups lane, lane+32, ...
+            // (channels 4g..4g+3), one 16-byte load per neighbour and group
+            const int G = a.V >> 2;
+            const float4* __restrict__ chan4 = reinterpret_cast<const float4*>(a.chan);
 #pragma unroll 1
-          for (int c = lane; c < a.V; c += 32) {
-            float ev[4];
+            for (int gi = lane; gi < G; gi += 32) {
+              float ev[4][4];
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-              float dot = 0.0f;
+              for (int p = 0; p < 4; ++p) {
+                float dot[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-              for (int q = 0; q < 8; ++q) {
-                const int id = S.id[p][q];
-                const float v = id >= 0 ? __ldg(&a.chan[(size_t)id * a.V + c]) : 0.0f;
-                dot = __fmaf_rn(S.w[p][q], v, dot);
+                for (int q = 0; q < 8; ++q) {
+                  const int id = S.id[p][q];
+                  const float4 v = id >= 0 ? __ldg(&chan4[(size_t)id * G + gi])
+                                           : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                  const float wq = S.w[p][q];
+                  dot[0] = __fmaf_rn(wq, v.x, dot[0]);
+                  dot[1] = __fmaf_rn(wq, v.y, dot[1]);
+                  dot[2] = __fmaf_rn(wq, v.z, dot[2]);
+                  dot[3] = __fmaf_rn(wq, v.w, dot[3]);
+                }
+                const float wsum = S.ws[p];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                  ev[p][k] = (wsum != 0.0f && dot[k] != 0.0f) ? dot[k] / wsum : 0.0f;
               }
-              const float wsum = S.ws[p];
-              ev[p] = (wsum != 0.0f && dot != 0.0f) ? dot / wsum : 0.0f;
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const int c = 4 * gi + k;
+                double x;
+                Es[c] = channel_step(Is[c], Ks[c], ev[0][k], ev[1][k], ev[2][k], ev[3][k], hd,
+                                     znew, a.atol, a.rtol, x);
+                E2s[c] = ev[2][k];
+                if (c == 0 && isnan(x)) x0nan = true;
+                xl = fmin(xl, x);
+              }
             }
-            const float Ic = Is[c], k1c = Ks[c];
-            double d4 = 25.0 / 216.0 * (double)k1c + 1408.0 / 2565.0 * (double)ev[0] +
-                        2197.0 / 4101.0 * (double)ev[1] - 1.0 / 5.0 * (double)ev[2];
-            double d5 = 16.0 / 135.0 * (double)k1c + 6656.0 / 12825.0 * (double)ev[0] +
-                        28561.0 / 56430.0 * (double)ev[1] - 9.0 / 50.0 * (double)ev[2] +
-                        2.0 / 55.0 * (double)ev[3];
-            d4 *= hd;
-            d5 *= hd;
-            Es[c] = (float)((double)Ic + d4);
-            E2s[c] = ev[2];
-            double x = 16.0;
-            if (d4 != d5) {
-              const double err = fabs(d5 - d4);
-              const double srt = fabs((double)Ic / (double)znew * a.rtol);
-              const double ot = fmax(a.atol, srt);
-              x = ot * hd / (2.0 * err);
+          } else {
+#pragma unroll 1
+            for (int c = lane; c < a.V; c += 32) {
+              float ev[4];
+#pragma unroll
+              for (int p = 0; p < 4; ++p) {
+                float dot = 0.0f;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                  const int id = S.id[p][q];
+                  const float v = id >= 0 ? __ldg(&a.chan[(size_t)id * a.V + c]) : 0.0f;
+                  dot = __fmaf_rn(S.w[p][q], v, dot);
+                }
+                const float wsum = S.ws[p];
+                ev[p] = (wsum != 0.0f && dot != 0.0f) ? dot / wsum : 0.0f;
+              }
+              double x;
+              Es[c] = channel_step(Is[c], Ks[c], ev[0], ev[1], ev[2], ev[3], hd, znew, a.atol,
+                                   a.rtol, x);
+              E2s[c] = ev[2];
+              if (c == 0 && isnan(x)) x0nan = true;
+              xl = fmin(xl, x);
             }
-            if (c == 0 && isnan(x)) x0nan = true;
-            xl = fmin(xl, x);
           }
 #pragma unroll
           for (int off = 16; off > 0; off >>= 1) xl = fmin(xl, __shfl_xor_sync(kFull, xl, off));
