@@ -126,22 +126,22 @@ def tune_schedule(ctx, cam, args, gpu_name):
         ctx.set_render_engine(ilc.ENGINE_PERSISTENT)
         key = base + "|persistent"
         if args.z_window is not None:
-            ctx.set_batch_schedule(8, 3, args.z_window, True)
-            return {"engine": "persistent", "tile_w": 8, "occupancy": 3,
+            ctx.set_batch_schedule(8, 4, args.z_window, True)
+            return {"engine": "persistent", "tile_w": 8, "occupancy": 4,
                     "z_window": args.z_window, "source": "command line"}
         if key in cache and not args.autotune:
             e = cache[key]
             ctx.set_batch_schedule(e["tile_w"], e["occupancy"], e["z_window"], True)
             return dict(e, engine="persistent", source="cache")
         if not args.autotune:
-            ctx.set_batch_schedule(8, 3, 40.0, True)
-            return {"engine": "persistent", "tile_w": 8, "occupancy": 3, "z_window": 40.0,
+            ctx.set_batch_schedule(8, 4, 40.0, True)
+            return {"engine": "persistent", "tile_w": 8, "occupancy": 4, "z_window": 40.0,
                     "source": "default"}
         half = ilc.camera(*camera_args()[:4], NX // 2, NY // 2)
         q = ctx.tuning_values
         bt, bo, bw, times = ctx.autotune_batched(q, [ilc.job(half, z_range=DEPTH)], REL_TOL, 0.0,
-                                                 tile_ws=(4, 8, 16, 32), occupancies=(0, 3),
-                                                 windows=(0.0, 20.0, 80.0))
+                                                 tile_ws=(8, 16, 32), occupancies=(4, 5),
+                                                 windows=(20.0, 80.0))
         cache[key] = {"tile_w": bt, "occupancy": bo, "z_window": bw,
                       "kernel_ms": {f"t{t}_o{o}_w{w}": v for (t, o, w), v in times.items()}}
         src = "autotuner"

@@ -149,7 +149,7 @@ class Context:
 
     def autotune_render(self, cam, z_range, rel_tol=1e-3, abs_tol=0.0,
                         controller=CONTROLLER_FP64, windows=(0, 5, 10, 20, 40, 80),
-                        occupancies=(0, 3, 4), sample_stride=16):
+                        occupancies=(0, 4, 5), sample_stride=16):
         """Times the adaptive render on a sample of tile rows for each
         (z window, occupancy) pair, sets the fastest on the context; returns
         (best window, best occupancy, {(window, occupancy): ms})."""
@@ -332,7 +332,7 @@ class Context:
         return img, g_r, g_t, st.as_dict()
 
     # ---- batched render
-    def set_batch_schedule(self, tile_w=8, blocks_per_sm=0, z_window=0.0, cost_order=True):
+    def set_batch_schedule(self, tile_w=8, blocks_per_sm=4, z_window=40.0, cost_order=True):
         self.check(self.L.ilc_set_batch_schedule(self.h, int(tile_w), int(blocks_per_sm),
                                                  float(z_window), 1 if cost_order else 0))
 
@@ -359,7 +359,7 @@ class Context:
         return images, st.as_dict()
 
     def autotune_batched(self, values, jobs, rel_tol=1e-3, abs_tol=0.0,
-                         tile_ws=(4, 8, 16, 32), occupancies=(0, 3, 4), windows=(0.0, 40.0)):
+                         tile_ws=(4, 8, 16, 32), occupancies=(0, 4, 5), windows=(0.0, 40.0)):
         """Times every (tile_w, occupancy, z_window) on the jobs, sets the
         fastest; returns (tile_w, occupancy, window, {(t, o, w): ms})."""
         dev = _is_dev(values)

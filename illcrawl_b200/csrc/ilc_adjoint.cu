@@ -166,14 +166,14 @@ __device__ __forceinline__ void scatter4(const Step4& s, float c, double* __rest
   float ws = 0.0f;
 #pragma unroll
   for (int t = 0; t < 8; ++t) {
-    w[t] = weight3d(s.d[J][t]);
+    w[t] = weight3d(s4_d(s, J, t));
     ws = ws + w[t];
   }
   if (!(ws > 0.0f) || !isfinite(ws)) return;
   const double f = (double)c / (double)ws;
 #pragma unroll
   for (int t = 0; t < 8; ++t) {
-    const int id = __float_as_int(s.v[J][t]);
+    const int id = __float_as_int(s4_v(s, J, t));
     if (id >= 0 && w[t] != 0.0f) atomicAdd(&grad[id], f * (double)w[t]);
   }
 }
@@ -204,8 +204,8 @@ __device__ __forceinline__ void scatter_prev(const PrevSlots& s, float c,
 __device__ __forceinline__ void keep_prev(const Step4& s, PrevSlots& p) {
 #pragma unroll
   for (int t = 0; t < 8; ++t) {
-    p.d[t] = s.d[2][t];
-    p.id[t] = __float_as_int(s.v[2][t]);
+    p.d[t] = s4_d(s, 2, t);
+    p.id[t] = __float_as_int(s4_v(s, 2, t));
   }
 }
 
@@ -214,14 +214,14 @@ template <int J>
 __device__ __forceinline__ float value_by_id(const Step4& s, const float4* __restrict__ parts) {
   float w[8];
 #pragma unroll
-  for (int t = 0; t < 8; ++t) w[t] = weight3d(s.d[J][t]);
+  for (int t = 0; t < 8; ++t) w[t] = weight3d(s4_d(s, J, t));
   float ws = 0.0f;
 #pragma unroll
   for (int t = 0; t < 8; ++t) ws = ws + w[t];
   float dot = 0.0f;
 #pragma unroll
   for (int t = 0; t < 8; ++t) {
-    const int id = __float_as_int(s.v[J][t]);
+    const int id = __float_as_int(s4_v(s, J, t));
     dot = __fmaf_rn(w[t], id >= 0 ? __ldg(&parts[id].w) : 0.0f, dot);
   }
   return (ws != 0.0f && dot != 0.0f) ? dot / ws : 0.0f;
@@ -245,6 +245,7 @@ __global__ void __launch_bounds__(128)
 adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
                uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
   __shared__ char4 spiral[1000];
+  __shared__ SlotMem slot_mem;
   load_spiral(spiral, spiral_g);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int ix = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
@@ -269,6 +270,7 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
       float p[4];
       rkf_points(z, h, p);
       Step4 s;
+      s4_bind(s, slot_mem);
       nn8_walk_step4<true>(g, spiral, px, py, pz, lx, ly, lz, p, s, ws);
       scatter4<0>(s, gi * (h * 1408.f / 2565.f), a.grad);
       scatter4<1>(s, gi * (h * 2197.f / 4101.f), a.grad);
@@ -288,6 +290,7 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
     while (z < a.z_end) {
       if ((int64_t)steps >= a.max_steps) { atomicOr(flags, FLAG_STEP_LIMIT); break; }
       Step4 s;
+      s4_bind(s, slot_mem);
       nn8_walk_step4<true>(g, spiral, px, py, pz, lx, ly, lz, pts, s, ws);
       const float e[4] = {value_by_id<0>(s, g.parts), value_by_id<1>(s, g.parts),
                           value_by_id<2>(s, g.parts), value_by_id<3>(s, g.parts)};

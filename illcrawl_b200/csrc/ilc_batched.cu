@@ -35,13 +35,6 @@ namespace {
 constexpr int kBThreads = 128;
 constexpr unsigned kFull = 0xffffffffu;
 
-// One ray's neighbour slots, handed from the walking lane to the warp.
-struct RaySlots {
-  int32_t id[4][8];
-  float w[4][8];
-  float ws[4];
-};
-
 struct BatchK {
   const JobDev* jobs;
   int n_jobs;
@@ -115,7 +108,7 @@ __device__ __forceinline__ void ray_span(const JobDev& j, int ix, int iy, bool& 
 template <int J>
 __device__ __forceinline__ void slot_weights(const Step4& s, float w[8], float& ws) {
 #pragma unroll
-  for (int t = 0; t < 8; ++t) w[t] = weight3d(s.d[J][t]);
+  for (int t = 0; t < 8; ++t) w[t] = weight3d(s4_d(s, J, t));
   ws = 0.0f;
 #pragma unroll
   for (int t = 0; t < 8; ++t) ws = ws + w[t];
@@ -131,23 +124,22 @@ __device__ __forceinline__ float value1(const Step4& s, const float* __restrict_
   float dot = 0.0f;
 #pragma unroll
   for (int t = 0; t < 8; ++t) {
-    const int id = __float_as_int(s.v[J][t]);
+    const int id = __float_as_int(s4_v(s, J, t));
     const float v = id < 0 ? 0.0f : (chan ? __ldg(&chan[id]) : __ldg(&parts[id].w));
     dot = __fmaf_rn(w[t], v, dot);
   }
   return (ws != 0.0f && dot != 0.0f) ? dot / ws : 0.0f;
 }
 
+// Hands point J's slots to the warp: the distances become weights in place
+// (the indices stay), and their sum goes to wsum.
 template <int J>
-__device__ __forceinline__ void store_slots(const Step4& s, RaySlots& r) {
+__device__ __forceinline__ void slots_to_weights(const Step4& s, float& wsum) {
   float w[8], ws;
   slot_weights<J>(s, w, ws);
 #pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    r.id[J][t] = __float_as_int(s.v[J][t]);
-    r.w[J][t] = w[t];
-  }
-  r.ws[J] = ws;
+  for (int t = 0; t < 8; ++t) s4_d(s, J, t) = w[t];
+  wsum = ws;
 }
 
 // One channel's FP64 step candidate: returns I + delta4 (as the accepted
@@ -177,7 +169,10 @@ __global__ void __launch_bounds__(kBThreads, kMinBlocks)
 batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
                uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
   __shared__ char4 spiral[1000];
-  __shared__ RaySlots slots[kMulti ? kBThreads : 1];
+  // slot arrays of the walks; for V > 1 also the hand-over to the warp:
+  // weights in the distance rows, indices in the value rows, sums in slot_ws
+  __shared__ SlotMem slot_mem;
+  __shared__ float slot_ws[kMulti ? 4 : 1][kBThreads];
   load_spiral(spiral, spiral_g);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tw = a.tile_w, th = 32 / a.tile_w;
@@ -226,6 +221,7 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
       const bool go = run && z < len && z < wend;
       if (go) {
         Step4 s;
+        s4_bind(s, slot_mem);
         nn8_walk_step4<true>(g, spiral, o[0], o[1], o[2], lx, ly, lz, pts, s, ws);
         if (!kMulti) {
           float e[4];
@@ -238,11 +234,10 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
           ++rs;
           if (z != zb) ++ra;
         } else {
-          RaySlots& r = slots[threadIdx.x];
-          store_slots<0>(s, r);
-          store_slots<1>(s, r);
-          store_slots<2>(s, r);
-          store_slots<3>(s, r);
+          slots_to_weights<0>(s, slot_ws[0][threadIdx.x]);
+          slots_to_weights<1>(s, slot_ws[1][threadIdx.x]);
+          slots_to_weights<2>(s, slot_ws[2][threadIdx.x]);
+          slots_to_weights<3>(s, slot_ws[3][threadIdx.x]);
         }
       }
       if (kMulti) {
@@ -254,7 +249,7 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
           const int r = __ffs(gom) - 1;
           gom &= gom - 1;
           const float zr = __shfl_sync(kFull, z, r), hr = __shfl_sync(kFull, h, r);
-          const RaySlots& S = slots[warp * 32 + r];
+          const int tr = warp * 32 + r;  // ray r's thread: its slot columns
           float* Is = wstate + (size_t)r * 4 * a.V;
           float* Ks = Is + a.V;
           const double hd = (double)hr;
@@ -278,16 +273,16 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
                 float dot[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
-                  const int id = S.id[p][q];
+                  const int id = __float_as_int(slot_mem.v[p * 8 + q][tr]);
                   const float4 v = id >= 0 ? __ldg(&chan4[(size_t)id * G + gi])
                                            : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                  const float wq = S.w[p][q];
+                  const float wq = slot_mem.d[p * 8 + q][tr];
                   dot[0] = __fmaf_rn(wq, v.x, dot[0]);
                   dot[1] = __fmaf_rn(wq, v.y, dot[1]);
                   dot[2] = __fmaf_rn(wq, v.z, dot[2]);
                   dot[3] = __fmaf_rn(wq, v.w, dot[3]);
                 }
-                const float wsum = S.ws[p];
+                const float wsum = slot_ws[p][tr];
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
                   ev[p][k] = (wsum != 0.0f && dot[k] != 0.0f) ? dot[k] / wsum : 0.0f;
@@ -312,11 +307,11 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
                 float dot = 0.0f;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
-                  const int id = S.id[p][q];
+                  const int id = __float_as_int(slot_mem.v[p * 8 + q][tr]);
                   const float v = id >= 0 ? __ldg(&a.chan[(size_t)id * a.V + c]) : 0.0f;
-                  dot = __fmaf_rn(S.w[p][q], v, dot);
+                  dot = __fmaf_rn(slot_mem.d[p * 8 + q][tr], v, dot);
                 }
-                const float wsum = S.ws[p];
+                const float wsum = slot_ws[p][tr];
                 ev[p] = (wsum != 0.0f && dot != 0.0f) ? dot / wsum : 0.0f;
               }
               double x;
@@ -464,10 +459,14 @@ cudaError_t launch_variant(Context& c, const BatchK& k, const GridView& g, int b
 
 int variant_blocks(const Context& c, bool multi, int occ) {
   if (multi)
-    return occ == 4 ? persistent_blocks<true, 4>(c)
-                    : occ == 3 ? persistent_blocks<true, 3>(c) : persistent_blocks<true, 1>(c);
-  return occ == 4 ? persistent_blocks<false, 4>(c)
-                  : occ == 3 ? persistent_blocks<false, 3>(c) : persistent_blocks<false, 1>(c);
+    return occ == 5   ? persistent_blocks<true, 5>(c)
+           : occ == 4 ? persistent_blocks<true, 4>(c)
+           : occ == 3 ? persistent_blocks<true, 3>(c)
+                      : persistent_blocks<true, 1>(c);
+  return occ == 5   ? persistent_blocks<false, 5>(c)
+         : occ == 4 ? persistent_blocks<false, 4>(c)
+         : occ == 3 ? persistent_blocks<false, 3>(c)
+                    : persistent_blocks<false, 1>(c);
 }
 
 cudaError_t enqueue(Context& c, const BatchK& k, const GridView& g, int occ, int blocks) {
@@ -475,10 +474,12 @@ cudaError_t enqueue(Context& c, const BatchK& k, const GridView& g, int occ, int
   if ((e = cudaMemsetAsync(c.flags.p, 0, kFlagsBytes, c.stream))) return e;
   if ((e = cudaMemsetAsync(c.queue.p, 0, 8, c.stream))) return e;
   if (k.V == 1)
-    return occ == 4   ? launch_variant<false, 4>(c, k, g, blocks)
+    return occ == 5   ? launch_variant<false, 5>(c, k, g, blocks)
+           : occ == 4 ? launch_variant<false, 4>(c, k, g, blocks)
            : occ == 3 ? launch_variant<false, 3>(c, k, g, blocks)
                       : launch_variant<false, 1>(c, k, g, blocks);
-  return occ == 4   ? launch_variant<true, 4>(c, k, g, blocks)
+  return occ == 5   ? launch_variant<true, 5>(c, k, g, blocks)
+         : occ == 4 ? launch_variant<true, 4>(c, k, g, blocks)
          : occ == 3 ? launch_variant<true, 3>(c, k, g, blocks)
                     : launch_variant<true, 1>(c, k, g, blocks);
 }

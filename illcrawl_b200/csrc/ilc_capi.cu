@@ -453,8 +453,8 @@ ilc_status ilc_set_render_engine(ilc_ctx* h, int32_t engine) {
 
 ilc_status ilc_set_render_occupancy(ilc_ctx* h, int32_t blocks_per_sm) {
   if (!h) return ILC_ERR_INVALID_ARGUMENT;
-  if (blocks_per_sm != 0 && blocks_per_sm != 3 && blocks_per_sm != 4)
-    return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3 or 4");
+  if (blocks_per_sm != 0 && blocks_per_sm != 3 && blocks_per_sm != 4 && blocks_per_sm != 5)
+    return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3, 4 or 5");
   h->c.render_occupancy = blocks_per_sm;
   return ILC_OK;
 }
@@ -939,8 +939,8 @@ ilc_status ilc_autotune_render(ilc_ctx* h, const ilc_camera* cam, double z_range
     if (!(windows[i] >= 0.0f) || !std::isfinite(windows[i]))
       return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z window candidate");
     for (int32_t j = 0; j < n_occupancies; ++j) {
-      if (occupancies[j] != 0 && occupancies[j] != 3 && occupancies[j] != 4)
-        return fail(c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3 or 4");
+      if (occupancies[j] != 0 && occupancies[j] != 3 && occupancies[j] != 4 && occupancies[j] != 5)
+        return fail(c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3, 4 or 5");
       a.window_override = windows[i];
       a.occupancy_override = occupancies[j];
       float ms = 0.0f;
@@ -1000,10 +1000,10 @@ ilc_status ilc_quantity_xray_spectrum(ilc_ctx* h, const float* rho, const float*
 ilc_status ilc_set_batch_schedule(ilc_ctx* h, int32_t tile_w, int32_t blocks_per_sm,
                                   float z_window, int32_t cost_order) {
   if (!h) return ILC_ERR_INVALID_ARGUMENT;
-  if (!tile_w_ok(tile_w) || (blocks_per_sm != 0 && blocks_per_sm != 3 && blocks_per_sm != 4) ||
+  if (!tile_w_ok(tile_w) || (blocks_per_sm != 0 && blocks_per_sm != 3 && blocks_per_sm != 4 && blocks_per_sm != 5) ||
       !(z_window >= 0.0f) || !std::isfinite(z_window))
     return fail(h->c, ILC_ERR_INVALID_ARGUMENT,
-                "tile_w in 1..32 (powers of 2), occupancy 0, 3 or 4, z_window >= 0");
+                "tile_w in 1..32 (powers of 2), occupancy 0, 3, 4 or 5, z_window >= 0");
   h->c.batch_tile_w = tile_w;
   h->c.batch_occupancy = blocks_per_sm;
   h->c.batch_window = z_window;
@@ -1064,8 +1064,8 @@ ilc_status ilc_autotune_batched(ilc_ctx* h, const float* values, int32_t n_chann
   for (int32_t i = 0; i < n_tiles; ++i)
     if (!tile_w_ok(tile_ws[i])) return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid tile_w");
   for (int32_t i = 0; i < n_occupancies; ++i)
-    if (occupancies[i] != 0 && occupancies[i] != 3 && occupancies[i] != 4)
-      return fail(c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3 or 4");
+    if (occupancies[i] != 0 && occupancies[i] != 3 && occupancies[i] != 4 && occupancies[i] != 5)
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "occupancy must be 0, 3, 4 or 5");
   for (int32_t i = 0; i < n_windows; ++i)
     if (!(windows[i] >= 0.0f) || !std::isfinite(windows[i]))
       return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z window");

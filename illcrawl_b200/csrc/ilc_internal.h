@@ -52,7 +52,7 @@ struct Context {
   std::string error;
   int64_t max_steps = 1 << 20;  // per-ray RKF step cap
   float z_window = 0.0f;        // adaptive render: z window of the block schedule (0 = none)
-  int32_t render_occupancy = 0; // adaptive render: blocks per SM (0 = register-limited)
+  int32_t render_occupancy = 4; // adaptive render: blocks per SM (0 = register-limited)
   int32_t render_engine = ILC_ENGINE_PERSISTENT;  // FP64 adaptive renders: kernel used
 
   // particle grid
@@ -89,8 +89,8 @@ struct Context {
   // batched render: job table, sorted channel table, channel state, queue
   DevBuf jobs, chan_sorted, chan_state, queue, item_cost, item_order;
   int32_t batch_tile_w = 8;       // batched work item: tile_w x (32 / tile_w) pixels
-  int32_t batch_occupancy = 0;    // batched kernel: blocks per SM (0 = register-limited)
-  float batch_window = 0.0f;      // batched kernel: per-warp z window (0 = none)
+  int32_t batch_occupancy = 4;    // batched kernel: blocks per SM (0 = register-limited)
+  float batch_window = 40.0f;     // batched kernel: per-warp z window (0 = none)
   bool batch_cost_order = true;   // hand out the costliest tiles first
   cudaGraphExec_t batch_exec = nullptr;  // the batched launch sequence as a CUDA graph
   std::string batch_key;                 // launch parameters it was captured with

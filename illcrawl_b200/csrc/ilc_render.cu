@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(kRenderThreads, kMinBlocks)
 render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
               uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
   __shared__ char4 spiral[1000];
+  __shared__ SlotMem slot_mem;
   load_spiral(spiral, spiral_g);
   int ix, iy;
   block_pixel(a.row_stride, ix, iy);
@@ -95,7 +96,7 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
         h = hs[s];
         rkf_points(z, h, pts);
         float e[4];
-        nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
+        nn8_step4(g, spiral, slot_mem, px, py, pz, lx, ly, lz, pts, e, ws);
         float d4 = 25.f / 216.f * k1 + 1408.f / 2565.f * e[0] + 2197.f / 4101.f * e[1] -
                    1.f / 5.f * e[2];
         d4 *= h;
@@ -112,7 +113,7 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
       for (int64_t s = 0; s < a.fixed_steps; ++s) {
         rkf_points(z, h, pts);
         float e[4];
-        nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
+        nn8_step4(g, spiral, slot_mem, px, py, pz, lx, ly, lz, pts, e, ws);
         float d4 = 25.f / 216.f * k1 + 1408.f / 2565.f * e[0] + 2197.f / 4101.f * e[1] -
                    1.f / 5.f * e[2];
         d4 *= h;
@@ -135,7 +136,7 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
       while (run && z < a.z_end && z < wend) {
         if ((int64_t)steps >= a.max_steps) { at_limit = true; run = false; break; }
         float e[4];
-        nn8_step4(g, spiral, px, py, pz, lx, ly, lz, pts, e, ws);
+        nn8_step4(g, spiral, slot_mem, px, py, pz, lx, ly, lz, pts, e, ws);
         const float zb = z, hb = h;
         if (a.controller == ILC_CONTROLLER_REF32)
           rkf_advance_ref32(I, z, h, k1, fa, fr, a.z_end, e, kEps, kHmin, kHmax, pts);
@@ -219,7 +220,10 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   ++c.launches;
   const int occ = a.occupancy_override >= 0 ? a.occupancy_override : c.render_occupancy;
   unsigned long long* stats = reinterpret_cast<unsigned long long*>(c.flags.as<char>() + 64);
-  if (occ == 4)
+  if (occ == 5)
+    render_kernel<5><<<grid, kRenderThreads, 0, c.stream>>>(k, g, c.spiral.as<char4>(),
+                                                            c.flags.as<uint32_t>(), stats);
+  else if (occ == 4)
     render_kernel<4><<<grid, kRenderThreads, 0, c.stream>>>(k, g, c.spiral.as<char4>(),
                                                             c.flags.as<uint32_t>(), stats);
   else if (occ == 3)

@@ -18,22 +18,48 @@
 
 namespace ilc {
 
+// Threads per block of every kernel that walks with Step4: the slot arrays of
+// thread i live in shared memory at index i of each of the 64 rows.
+constexpr int kSlotThreads = 128;
+constexpr int kSlotRows = 4 * 8;  // (point, slot) pairs
+
+// Shared-memory storage of one block's slot arrays: distance rows, then value
+// (or index) rows; row (j, t) holds entry t of point j for all threads.
+struct SlotMem {
+  float d[kSlotRows][kSlotThreads];
+  float v[kSlotRows][kSlotThreads];
+};
+
 struct Step4 {
   float qx[4], qy[4], qz[4];
-  float d[4][8], v[4][8];
+  float* sd;      // this thread's distance column: sd[(j * 8 + t) * kSlotThreads]
+  float* sv;      // this thread's value column
   float R[4], R2up[4];
   float rr[4];    // (R + cell_radius)^2: the early-break threshold
   float crad;     // cell radius
-  int mi[4], cnt[4];
+  int mi[4];      // first maximal slot; while R == FLT_MAX: the next empty slot
 };
+
+__device__ __forceinline__ float& s4_d(const Step4& s, int j, int t) {
+  return s.sd[(j * 8 + t) * kSlotThreads];
+}
+__device__ __forceinline__ float& s4_v(const Step4& s, int j, int t) {
+  return s.sv[(j * 8 + t) * kSlotThreads];
+}
+
+__device__ __forceinline__ void s4_bind(Step4& s, SlotMem& m) {
+  s.sd = &m.d[0][threadIdx.x];
+  s.sv = &m.v[0][threadIdx.x];
+}
 
 template <int J> __device__ __forceinline__ void s4_rescan(Step4& s) {
   float r = 0.0f;
   int m = 0;
 #pragma unroll
   for (int t = 0; t < 8; ++t) {
-    if (s.d[J][t] > r) m = t;
-    r = fmaxf(r, s.d[J][t]);
+    const float d = s4_d(s, J, t);
+    if (d > r) m = t;
+    r = fmaxf(r, d);
   }
   s.R[J] = r;
   s.mi[J] = m;
@@ -42,34 +68,32 @@ template <int J> __device__ __forceinline__ void s4_rescan(Step4& s) {
   s.rr[J] = b * b;
 }
 
-template <int J> __device__ __forceinline__ void s4_init(Step4& s) {
+template <int J> __device__ __forceinline__ void s4_init(Step4& s, float empty_value) {
 #pragma unroll
-  for (int t = 0; t < 8; ++t) { s.d[J][t] = FLT_MAX; s.v[J][t] = 0.0f; }
+  for (int t = 0; t < 8; ++t) {
+    s4_d(s, J, t) = FLT_MAX;
+    s4_v(s, J, t) = empty_value;
+  }
   s.R[J] = FLT_MAX;
   s.R2up[J] = __int_as_float(0x7f800000);
   const float b = FLT_MAX + s.crad;
   s.rr[J] = b * b;
   s.mi[J] = 0;
-  s.cnt[J] = 0;
 }
 
 // Insertion into point J's slots. While fewer than 8 slots are filled the
-// search radius is FLT_MAX and the first-max slot is the next empty one, so
-// the k-th accepted candidate goes to slot k without a rescan; the 8th
-// insertion rescans. Afterwards: replace the first-max slot and rescan.
+// search radius is FLT_MAX (a full set of 8 finite distances makes it
+// smaller) and the first-max slot is the next empty one, so the k-th
+// accepted candidate goes to slot k without a rescan; the 8th insertion
+// rescans. Afterwards: replace the first-max slot and rescan.
 template <int J> __device__ __forceinline__ void s4_insert(Step4& s, float dist, float val) {
-  if (s.cnt[J] < 8) {
-    const int k = s.cnt[J];
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (t == k) { s.d[J][t] = dist; s.v[J][t] = val; }
-    s.cnt[J] = k + 1;
+  const int k = s.mi[J];
+  s4_d(s, J, k) = dist;
+  s4_v(s, J, k) = val;
+  if (s.R[J] == FLT_MAX) {
+    s.mi[J] = k + 1;
     if (k == 7) s4_rescan<J>(s);
   } else {
-    const int m = s.mi[J];
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (t == m) { s.d[J][t] = dist; s.v[J][t] = val; }
     s4_rescan<J>(s);
   }
 }
@@ -87,13 +111,13 @@ __device__ __forceinline__ void s4_test(Step4& s, unsigned act, float d2, float 
 template <int J> __device__ __forceinline__ float s4_finalize(const Step4& s) {
   float w[8];
 #pragma unroll
-  for (int t = 0; t < 8; ++t) w[t] = weight3d(s.d[J][t]);
+  for (int t = 0; t < 8; ++t) w[t] = weight3d(s4_d(s, J, t));
   float ws = 0.0f;
 #pragma unroll
   for (int t = 0; t < 8; ++t) ws = ws + w[t];
   float dot = 0.0f;
 #pragma unroll
-  for (int t = 0; t < 8; ++t) dot = __fmaf_rn(w[t], s.v[J][t], dot);
+  for (int t = 0; t < 8; ++t) dot = __fmaf_rn(w[t], s4_v(s, J, t), dot);
   float res = 0.0f;
   if (ws != 0.0f && dot != 0.0f) res = dot / ws;
   return res;
@@ -298,16 +322,11 @@ __device__ __forceinline__ void nn8_walk_step4(const GridView& g,
     locate(g, s.qx[j], s.qy[j], s.qz[j], cx[j], cy[j], cz[j], sb[j]);
   }
   s.crad = g.cell_radius;
-  s4_init<0>(s);
-  s4_init<1>(s);
-  s4_init<2>(s);
-  s4_init<3>(s);
-  if (kIdx) {  // empty slots carry index -1
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int t = 0; t < 8; ++t) s.v[j][t] = __int_as_float(-1);
-  }
+  const float empty = kIdx ? __int_as_float(-1) : 0.0f;  // empty slots carry index -1
+  s4_init<0>(s, empty);
+  s4_init<1>(s, empty);
+  s4_init<2>(s, empty);
+  s4_init<3>(s, empty);
   const bool shared_xy = s.qx[0] == s.qx[1] && s.qx[0] == s.qx[2] && s.qx[0] == s.qx[3] &&
                          s.qy[0] == s.qy[1] && s.qy[0] == s.qy[2] && s.qy[0] == s.qy[3];
   unsigned todo = 0xFu;
@@ -332,10 +351,11 @@ __device__ __forceinline__ void nn8_walk_step4(const GridView& g,
 
 // nn8 values of the 4 points of one step (e[j] for point j).
 __device__ __forceinline__ void nn8_step4(const GridView& g, const char4* __restrict__ spiral,
-                                          float px, float py, float pz, float lx, float ly,
-                                          float lz, const float zq[4], float e[4],
+                                          SlotMem& sm, float px, float py, float pz, float lx,
+                                          float ly, float lz, const float zq[4], float e[4],
                                           WalkStats& st) {
   Step4 s;
+  s4_bind(s, sm);
   nn8_walk_step4<false>(g, spiral, px, py, pz, lx, ly, lz, zq, s, st);
   e[0] = s4_finalize<0>(s);
   e[1] = s4_finalize<1>(s);

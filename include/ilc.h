@@ -120,8 +120,8 @@ enum { ILC_ENGINE_GRID = 0, ILC_ENGINE_PERSISTENT = 1 };
 ilc_status ilc_set_render_engine(ilc_ctx* ctx, int32_t engine);
 
 /* Occupancy of the adaptive render: 0 = as many blocks per SM as the
- * kernel's registers allow, 3 or 4 = that many 128-thread blocks per SM
- * (registers capped, some spilled). Changes the order of work only, never a
+ * kernel's registers allow, 3, 4 or 5 = that many 128-thread blocks per SM
+ * (registers capped accordingly). Changes the order of work only, never a
  * result. */
 ilc_status ilc_set_render_occupancy(ilc_ctx* ctx, int32_t blocks_per_sm);
 
@@ -307,12 +307,12 @@ ilc_status ilc_render_batched(ilc_ctx* ctx, const float* values, int32_t n_chann
 
 /* Schedule of ilc_render_batched: work items are tiles of tile_w x
  * (32 / tile_w) pixels (tile_w in 1, 2, 4, 8, 16, 32), one per warp; 0
- * (register-limited), 3 or 4 blocks per SM; z_window > 0 makes a warp's rays
+ * (register-limited), 3, 4 or 5 blocks per SM; z_window > 0 makes a warp's rays
  * advance in windows of that depth (they query one slab of the grid at a
  * time); cost_order != 0 hands out the tiles in decreasing order of an
  * estimated cost (particles projected into each tile's columns, weighted by
  * their cell's occupancy), so the longest rays start first. Changes the order
- * of work only, never a result. Default: 8, 0, 0, 1. */
+ * of work only, never a result. Default: 8, 4, 40, 1. */
 ilc_status ilc_set_batch_schedule(ilc_ctx* ctx, int32_t tile_w, int32_t blocks_per_sm,
                                   float z_window, int32_t cost_order);
 

@@ -108,7 +108,7 @@ def test_batched_schedule_is_result_neutral(ctx):
     ref = None
     try:
         for tw, occ, win, order in ((8, 0, 0.0, False), (1, 0, 0.0, True), (4, 3, 25.0, True),
-                                    (8, 4, 7.0, True), (32, 0, 60.0, False), (16, 3, 0.0, True)):
+                                    (8, 4, 7.0, True), (32, 5, 60.0, False), (16, 3, 0.0, True)):
             ctx.set_batch_schedule(tw, occ, win, order)
             out, _ = ctx.render_batched(vals, _jobs(ilc, np.random.default_rng(3), sizes))
             if ref is None:

@@ -196,14 +196,14 @@ def test_autotuner_picks_a_candidate_and_keeps_results(ctx, oracle_mod):
     ctx.setup_particles(pts)
     args = ((500, 500, 0), (0, 0, 1), 0.0, 1000.0, 64, 64)
     bw, bo, times = ctx.autotune_render(ilc.camera(*args), 1000.0, 1e-3, windows=(0, 8, 32),
-                                        occupancies=(0, 3, 4), sample_stride=2)
+                                        occupancies=(0, 4, 5), sample_stride=2)
     try:
-        assert bw in (0.0, 8.0, 32.0) and bo in (0, 3, 4) and all(t > 0 for t in times.values())
+        assert bw in (0.0, 8.0, 32.0) and bo in (0, 4, 5) and all(t > 0 for t in times.values())
         assert times[(bw, bo)] == min(times.values())
         img, _ = ctx.render_adaptive(ilc.camera(*args), 1000.0, 1e-3, 0.0, 1)
     finally:
         ctx.set_z_window(0.0)
-        ctx.set_render_occupancy(0)
+        ctx.set_render_occupancy(4)
     out, *_ = oracle_mod.Grid(pts).render(oracle_mod.camera(*args), 1000.0, 0.0, 1e-3, mode=1,
                                           pix=np.arange(0, 64 * 64, 97))
     assert np.array_equal(img.ravel()[::97].view(np.uint32), out.view(np.uint32))
