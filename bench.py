@@ -140,7 +140,7 @@ def tune_schedule(ctx, cam, args, gpu_name):
         half = ilc.camera(*camera_args()[:4], NX // 2, NY // 2)
         q = ctx.tuning_values
         bt, bo, bw, times = ctx.autotune_batched(q, [ilc.job(half, z_range=DEPTH)], REL_TOL, 0.0,
-                                                 tile_ws=(8, 16, 32), occupancies=(4, 5),
+                                                 tile_ws=(0, 4, 8), occupancies=(4, 5),
                                                  windows=(20.0, 80.0))
         cache[key] = {"tile_w": bt, "occupancy": bo, "z_window": bw,
                       "kernel_ms": {f"t{t}_o{o}_w{w}": v for (t, o, w), v in times.items()}}

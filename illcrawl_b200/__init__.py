@@ -359,7 +359,7 @@ class Context:
         return images, st.as_dict()
 
     def autotune_batched(self, values, jobs, rel_tol=1e-3, abs_tol=0.0,
-                         tile_ws=(4, 8, 16, 32), occupancies=(0, 4, 5), windows=(0.0, 40.0)):
+                         tile_ws=(0, 4, 8, 16, 32), occupancies=(0, 4, 5), windows=(0.0, 40.0)):
         """Times every (tile_w, occupancy, z_window) on the jobs, sets the
         fastest; returns (tile_w, occupancy, window, {(t, o, w): ms})."""
         dev = _is_dev(values)

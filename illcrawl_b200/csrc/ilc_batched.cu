@@ -175,7 +175,7 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
   __shared__ float slot_ws[kMulti ? 4 : 1][kBThreads];
   load_spiral(spiral, spiral_g);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int tw = a.tile_w, th = 32 / a.tile_w;
+  const int tw = a.tile_w, th = a.tile_w > 0 ? 32 / a.tile_w : 1;
   unsigned long long t_steps = 0, t_acc = 0, t_cells = 0, t_cands = 0, t_max = 0, t_lim = 0;
   float* wstate = kMulti ? a.state + ((size_t)blockIdx.x * kBThreads + (size_t)warp * 32) *
                                          4 * (size_t)a.V
@@ -188,9 +188,19 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
     if (a.order) item = a.order[item];
     const JobDev& J = a.jobs[find_job(a.jobs, a.n_jobs, item)];
     const uint64_t t = item - J.item_begin;
-    const int tx = (int)(t % (uint64_t)J.tiles_x), ty = (int)(t / (uint64_t)J.tiles_x);
-    const int ix = tx * tw + lane % tw, iy = ty * th + lane / tw;
-    const bool inside = ix < J.nx && iy < J.ny;
+    int ix, iy;
+    bool inside;
+    if (tw > 0) {  // compact tile of tw x th pixels
+      const int tx = (int)(t % (uint64_t)J.tiles_x), ty = (int)(t / (uint64_t)J.tiles_x);
+      ix = tx * tw + lane % tw;
+      iy = ty * th + lane / tw;
+      inside = ix < J.nx && iy < J.ny;
+    } else {       // strided: pixels t, t + T, t + 2T, ... (T = items of the job)
+      const uint64_t pix = t + (uint64_t)lane * (uint64_t)J.tiles_x;
+      inside = pix < (uint64_t)J.nx * (uint64_t)J.ny;
+      ix = inside ? (int)(pix % (uint64_t)J.nx) : J.nx;
+      iy = inside ? (int)(pix / (uint64_t)J.nx) : J.ny;
+    }
     bool masked = true;
     float o[3] = {0.0f, 0.0f, 0.0f}, len = 0.0f;
     if (inside) ray_span(J, ix, iy, masked, o, len);
@@ -433,8 +443,9 @@ __global__ void tile_cost_kernel(const float4* __restrict__ parts,
     if (!(t >= 0.0f) || (!(J.radius > 0.0) && !(t <= (float)J.z_range))) continue;
     const int ix = (int)u, iy = (int)v;
     const int2 be = cells[keys[i]];
-    atomicAdd(&cost[J.item_begin + (uint64_t)(iy / th) * J.tiles_x + (uint64_t)(ix / tw)],
-              (float)(be.y - be.x));
+    const uint64_t item = tw > 0 ? (uint64_t)(iy / th) * J.tiles_x + (uint64_t)(ix / tw)
+                                 : ((uint64_t)iy * J.nx + ix) % (uint64_t)J.tiles_x;
+    atomicAdd(&cost[J.item_begin + item], (float)(be.y - be.x));
   }
 }
 
@@ -500,7 +511,7 @@ cudaError_t batched_order(Context& c, BatchArgs& a, const std::vector<JobDev>& j
   const uint64_t m = a.n_items;
   if ((e = c.item_cost.ensure(m * 4)) || (e = c.item_order.ensure(m * 4))) return e;
   if ((e = cudaMemsetAsync(c.item_cost.p, 0, m * 4, c.stream))) return e;
-  const int tw = a.tile_w, th = 32 / a.tile_w;
+  const int tw = a.tile_w, th = a.tile_w > 0 ? 32 / a.tile_w : 1;
   const uint64_t n = c.n_particles;
   const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 8);
   for (const JobDev& j : jobs) {

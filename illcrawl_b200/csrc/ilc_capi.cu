@@ -210,7 +210,7 @@ ilc_status batched_jobs(Context& c, int32_t V, const ilc_job* jobs, int32_t n_jo
     return fail(c, ILC_ERR_INVALID_ARGUMENT,
                 "either the absolute or the relative tolerance has to be > 0");
   std::vector<JobDev> jd((size_t)n_jobs);
-  const int tw = c.batch_tile_w, th = 32 / c.batch_tile_w;
+  const int tw = c.batch_tile_w, th = c.batch_tile_w > 0 ? 32 / c.batch_tile_w : 1;
   uint64_t items = 0;
   for (int32_t k = 0; k < n_jobs; ++k) {
     const ilc_job& j = jobs[k];
@@ -244,7 +244,9 @@ ilc_status batched_jobs(Context& c, int32_t V, const ilc_job* jobs, int32_t n_jo
     d.ps_d = dd[12];
     d.nx = j.camera.num_pix_x;
     d.ny = j.camera.num_pix_y;
-    d.tiles_x = (d.nx + tw - 1) / tw;
+    // compact tiles: tiles per row; strided (tw = 0): items of the job
+    const uint64_t npix = (uint64_t)d.nx * (uint64_t)d.ny;
+    d.tiles_x = tw > 0 ? (d.nx + tw - 1) / tw : (int32_t)((npix + 31) / 32);
     d.z_range = j.z_range;
     d.aperture = j.aperture_radius;
     d.radius = j.sphere_radius;
@@ -252,7 +254,8 @@ ilc_status batched_jobs(Context& c, int32_t V, const ilc_job* jobs, int32_t n_jo
     d.scale = j.scale;
     d.out_offset = j.out_offset;
     d.item_begin = items;
-    items += (uint64_t)d.tiles_x * (uint64_t)((d.ny + th - 1) / th);
+    items += tw > 0 ? (uint64_t)d.tiles_x * (uint64_t)((d.ny + th - 1) / th)
+                    : (uint64_t)d.tiles_x;
   }
   ILC_CUDA(c, c.jobs.ensure(jd.size() * sizeof(JobDev)), "job table");
   ILC_CUDA(c, cudaMemcpyAsync(c.jobs.p, jd.data(), jd.size() * sizeof(JobDev),
@@ -290,7 +293,9 @@ ilc_status batched_prepare(Context& c, const float* values, int32_t V, int value
   return ILC_OK;
 }
 
-bool tile_w_ok(int32_t w) { return w == 1 || w == 2 || w == 4 || w == 8 || w == 16 || w == 32; }
+bool tile_w_ok(int32_t w) {
+  return w == 0 || w == 1 || w == 2 || w == 4 || w == 8 || w == 16 || w == 32;
+}
 
 // Optional frozen replay (replay_h/replay_n) or step recording (rec_h/rec_n),
 // both device arrays of cap steps per ray; either forces the grid kernel.
@@ -1003,7 +1008,7 @@ ilc_status ilc_set_batch_schedule(ilc_ctx* h, int32_t tile_w, int32_t blocks_per
   if (!tile_w_ok(tile_w) || (blocks_per_sm != 0 && blocks_per_sm != 3 && blocks_per_sm != 4 && blocks_per_sm != 5) ||
       !(z_window >= 0.0f) || !std::isfinite(z_window))
     return fail(h->c, ILC_ERR_INVALID_ARGUMENT,
-                "tile_w in 1..32 (powers of 2), occupancy 0, 3, 4 or 5, z_window >= 0");
+                "tile_w 0 or 1..32 (powers of 2), occupancy 0, 3, 4 or 5, z_window >= 0");
   h->c.batch_tile_w = tile_w;
   h->c.batch_occupancy = blocks_per_sm;
   h->c.batch_window = z_window;

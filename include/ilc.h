@@ -306,7 +306,9 @@ ilc_status ilc_render_batched(ilc_ctx* ctx, const float* values, int32_t n_chann
                               int images_on_device, ilc_render_stats* stats);
 
 /* Schedule of ilc_render_batched: work items are tiles of tile_w x
- * (32 / tile_w) pixels (tile_w in 1, 2, 4, 8, 16, 32), one per warp; 0
+ * (32 / tile_w) pixels (tile_w in 1, 2, 4, 8, 16, 32), one per warp, or with
+ * tile_w = 0 strided items (pixels k, k + T, k + 2T, ... of a job with T items,
+ * which spreads the expensive rays of a small region over many warps); 0
  * (register-limited), 3, 4 or 5 blocks per SM; z_window > 0 makes a warp's rays
  * advance in windows of that depth (they query one slab of the grid at a
  * time); cost_order != 0 hands out the tiles in decreasing order of an

@@ -107,7 +107,7 @@ def test_batched_schedule_is_result_neutral(ctx):
     sizes = [(19, 11), (8, 8), (33, 5)]
     ref = None
     try:
-        for tw, occ, win, order in ((8, 0, 0.0, False), (1, 0, 0.0, True), (4, 3, 25.0, True),
+        for tw, occ, win, order in ((8, 0, 0.0, False), (1, 0, 0.0, True), (0, 3, 25.0, True),
                                     (8, 4, 7.0, True), (32, 5, 60.0, False), (16, 3, 0.0, True)):
             ctx.set_batch_schedule(tw, occ, win, order)
             out, _ = ctx.render_batched(vals, _jobs(ilc, np.random.default_rng(3), sizes))
