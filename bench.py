@@ -152,6 +152,19 @@ def tune_schedule(ctx, cam, args, gpu_name):
     return dict(cache[key], engine=args.engine, source=src)
 
 
+def measured_traffic(args):
+    """DRAM bytes (read + write) of one render launch of this workload, from
+    the committed ncu capture of the same bench command (profiles/); None for
+    other workloads or engines."""
+    p = os.path.join(ROOT, "profiles", "batched_kernel_xray_band_map_1024sq_traffic.json")
+    if args.engine != "persistent" or NX != 1024 or Z_START != 0.0 or DEPTH != BOX:
+        return None
+    try:
+        return int(json.load(open(p))["dram_bytes_per_launch"])
+    except (OSError, ValueError, KeyError):
+        return None
+
+
 def max_over_ranks(value, device):
     """The slowest rank's time (every rank takes this collective in the same
     order). Replicas share nothing else: no data-path collective."""
@@ -462,7 +475,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(28 * n),
                 "d2h_bytes_per_step": int(4 * NX * NY)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm, "traffic": measured_traffic(args),
                      "peak_kind": peak_kind,
                      "kernel": "batched_kernel" if args.engine == "persistent" else "render_kernel",
                      "kernel_ms": last_stats["kernel_ms"], "algorithmic_bytes": kbytes},
