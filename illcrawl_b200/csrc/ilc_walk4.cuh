@@ -98,12 +98,17 @@ template <int J> __device__ __forceinline__ void s4_insert(Step4& s, float dist,
   }
 }
 
+// Candidate test of point J against its threshold thr: R2up (R*R rounded up:
+// a squared distance above it cannot give dist < R) while J takes part in the
+// walk, -1 once it has left it (no squared distance passes). thr follows R2up
+// through insertions.
 template <int J>
-__device__ __forceinline__ void s4_test(Step4& s, unsigned act, float d2, float val) {
-  if ((act >> J) & 1u) {
-    if (d2 <= s.R2up[J]) {
-      const float dist = sqrtf(d2);
-      if (dist < s.R[J]) s4_insert<J>(s, dist, val);
+__device__ __forceinline__ void s4_test(Step4& s, float& thr, float d2, float val) {
+  if (d2 <= thr) {
+    const float dist = sqrtf(d2);
+    if (dist < s.R[J]) {
+      s4_insert<J>(s, dist, val);
+      thr = s.R2up[J];
     }
   }
 }
@@ -125,7 +130,7 @@ template <int J> __device__ __forceinline__ float s4_finalize(const Step4& s) {
 
 // Distance tests of one candidate against the active points.
 template <bool kSharedXY, bool kIdx>
-__device__ __forceinline__ void test_candidate(Step4& s, unsigned act, const float4& P, int p) {
+__device__ __forceinline__ void test_candidate(Step4& s, float thr[4], const float4& P, int p) {
   float d2[4];
   if (kSharedXY) {
     const float fx = P.x - s.qx[0], fy = P.y - s.qy[0];
@@ -143,10 +148,10 @@ __device__ __forceinline__ void test_candidate(Step4& s, unsigned act, const flo
     }
   }
   const float pay = kIdx ? __int_as_float(p) : P.w;
-  s4_test<0>(s, act, d2[0], pay);
-  s4_test<1>(s, act, d2[1], pay);
-  s4_test<2>(s, act, d2[2], pay);
-  s4_test<3>(s, act, d2[3], pay);
+  s4_test<0>(s, thr[0], d2[0], pay);
+  s4_test<1>(s, thr[1], d2[1], pay);
+  s4_test<2>(s, thr[2], d2[2], pay);
+  s4_test<3>(s, thr[3], d2[3], pay);
 }
 
 // Cells with more candidates than this are scanned through their sub-box codes.
@@ -198,6 +203,9 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
                                       WalkStats& st) {
   const char4* order = spiral + sub * 125;
   unsigned act = mask;
+  float thr[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) thr[j] = ((mask >> j) & 1u) ? s.R2up[j] : -1.0f;
   // bounding box of the group's points (for the sub-box pruning)
   float qlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, qhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
 #pragma unroll
@@ -232,13 +240,16 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
         }
       }
       act &= ~brk;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if ((brk >> j) & 1u) thr[j] = -1.0f;
     }
     if (!act) break;
     if ((unsigned)ix >= (unsigned)g.n0 || (unsigned)iy >= (unsigned)g.n1 ||
         (unsigned)iz >= (unsigned)g.n2)
       continue;
-    const size_t key = (size_t)ix + (size_t)iy * (size_t)g.n0 +
-                       (size_t)iz * (size_t)g.n0 * (size_t)g.n1;
+    // ix + iy nx + iz nx ny, in 32 bits (the grid build rejects 2^32 cells or more)
+    const uint32_t key = (uint32_t)ix + (uint32_t)g.n0 * ((uint32_t)iy + (uint32_t)g.n1 * (uint32_t)iz);
     const int2 be = __ldg(&g.cells[key]);
     const unsigned na = __popc(act);
     st.cells += na;
@@ -275,7 +286,7 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
         while (hits) {
           const int p = pw + __ffs(hits) - 1;
           hits &= hits - 1;
-          test_candidate<kSharedXY, kIdx>(s, act, __ldg(&g.parts[p]), p);
+          test_candidate<kSharedXY, kIdx>(s, thr, __ldg(&g.parts[p]), p);
         }
       }
       continue;
@@ -283,7 +294,7 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     float4 P = __ldg(&g.parts[be.x]);
     for (int p = be.x; p < be.y; ++p) {
       const float4 N = (p + 1 < be.y) ? __ldg(&g.parts[p + 1]) : P;  // prefetch
-      test_candidate<kSharedXY, kIdx>(s, act, P, p);
+      test_candidate<kSharedXY, kIdx>(s, thr, P, p);
       P = N;
     }
   }
