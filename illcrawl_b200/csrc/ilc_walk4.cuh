@@ -129,9 +129,8 @@ template <int J> __device__ __forceinline__ float s4_finalize(const Step4& s) {
 }
 
 // Distance tests of one candidate against the active points.
-template <bool kSharedXY, bool kIdx>
-__device__ __forceinline__ void test_candidate(Step4& s, float thr[4], const float4& P, int p) {
-  float d2[4];
+template <bool kSharedXY>
+__device__ __forceinline__ void cand_d2(const Step4& s, const float4& P, float d2[4]) {
   if (kSharedXY) {
     const float fx = P.x - s.qx[0], fy = P.y - s.qy[0];
     const float fxy = fx * fx + fy * fy;
@@ -147,11 +146,23 @@ __device__ __forceinline__ void test_candidate(Step4& s, float thr[4], const flo
       d2[j] = (fx * fx + fy * fy) + fz * fz;
     }
   }
+}
+
+template <bool kIdx>
+__device__ __forceinline__ void cand_insert(Step4& s, float thr[4], const float d2[4],
+                                            const float4& P, int p) {
   const float pay = kIdx ? __int_as_float(p) : P.w;
   s4_test<0>(s, thr[0], d2[0], pay);
   s4_test<1>(s, thr[1], d2[1], pay);
   s4_test<2>(s, thr[2], d2[2], pay);
   s4_test<3>(s, thr[3], d2[3], pay);
+}
+
+template <bool kSharedXY, bool kIdx>
+__device__ __forceinline__ void test_candidate(Step4& s, float thr[4], const float4& P, int p) {
+  float d2[4];
+  cand_d2<kSharedXY>(s, P, d2);
+  cand_insert<kIdx>(s, thr, d2, P, p);
 }
 
 // Cells with more candidates than this are scanned through their sub-box codes.
@@ -291,12 +302,18 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
       }
       continue;
     }
-    float4 P = __ldg(&g.parts[be.x]);
-    for (int p = be.x; p < be.y; ++p) {
-      const float4 N = (p + 1 < be.y) ? __ldg(&g.parts[p + 1]) : P;  // prefetch
-      test_candidate<kSharedXY, kIdx>(s, thr, P, p);
-      P = N;
+    // two candidates per iteration: both loads and both distance sets are
+    // independent; the insertions still run in index order
+    int p = be.x;
+    for (; p + 1 < be.y; p += 2) {
+      const float4 A = __ldg(&g.parts[p]), B = __ldg(&g.parts[p + 1]);
+      float da[4], db[4];
+      cand_d2<kSharedXY>(s, A, da);
+      cand_d2<kSharedXY>(s, B, db);
+      cand_insert<kIdx>(s, thr, da, A, p);
+      cand_insert<kIdx>(s, thr, db, B, p + 1);
     }
+    if (p < be.y) test_candidate<kSharedXY, kIdx>(s, thr, __ldg(&g.parts[p]), p);
   }
 }
 
