@@ -302,18 +302,12 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
       }
       continue;
     }
-    // two candidates per iteration: both loads and both distance sets are
-    // independent; the insertions still run in index order
-    int p = be.x;
-    for (; p + 1 < be.y; p += 2) {
-      const float4 A = __ldg(&g.parts[p]), B = __ldg(&g.parts[p + 1]);
-      float da[4], db[4];
-      cand_d2<kSharedXY>(s, A, da);
-      cand_d2<kSharedXY>(s, B, db);
-      cand_insert<kIdx>(s, thr, da, A, p);
-      cand_insert<kIdx>(s, thr, db, B, p + 1);
+    float4 P = __ldg(&g.parts[be.x]);
+    for (int p = be.x; p < be.y; ++p) {
+      const float4 N = (p + 1 < be.y) ? __ldg(&g.parts[p + 1]) : P;  // prefetch
+      test_candidate<kSharedXY, kIdx>(s, thr, P, p);
+      P = N;
     }
-    if (p < be.y) test_candidate<kSharedXY, kIdx>(s, thr, __ldg(&g.parts[p]), p);
   }
 }
 
