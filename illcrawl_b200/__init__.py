@@ -331,6 +331,23 @@ class Context:
             _ptr(g_r), _ptr(g_t), 0, ctypes.byref(st)))
         return img, g_r, g_t, st.as_dict()
 
+    # ---- cell ingestion
+    def ingest_cells(self, xyz, q, center, extent, periodic, border=100.0):
+        """Periodic correction + cutout + compaction (ilc_ingest_cells). Host
+        arrays in, host arrays out: (xyzq (m, 4), input indices (m,))."""
+        xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+        n = xyz.shape[0]
+        qa = None if q is None else np.ascontiguousarray(q, np.float32)
+        out = np.zeros((n, 4), np.float32)
+        idx = np.zeros(n, np.uint32)
+        m = ctypes.c_uint64(0)
+        c3 = lambda v: (ctypes.c_double * 3)(*[float(x) for x in v])
+        self.check(self.L.ilc_ingest_cells(self.h, _ptr(xyz), _ptr(qa), n, c3(center), c3(extent),
+                                           c3(periodic), float(border), _ptr(out), _ptr(idx),
+                                           ctypes.byref(m), 0))
+        k = int(m.value)
+        return out[:k], idx[:k]
+
     # ---- batched render
     def set_batch_schedule(self, tile_w=8, blocks_per_sm=4, z_window=40.0, cost_order=True):
         self.check(self.L.ilc_set_batch_schedule(self.h, int(tile_w), int(blocks_per_sm),

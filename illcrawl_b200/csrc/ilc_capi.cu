@@ -1138,4 +1138,58 @@ ilc_status ilc_autotune_batched(ilc_ctx* h, const float* values, int32_t n_chann
   return ILC_OK;
 }
 
+
+ilc_status ilc_ingest_cells(ilc_ctx* h, const float* xyz, const float* q, uint64_t n,
+                            const double* center, const double* extent, const double* periodic,
+                            double border, float* out_xyzq, uint32_t* out_index,
+                            uint64_t* n_out, int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!n_out) return fail(c, ILC_ERR_INVALID_ARGUMENT, "n_out is NULL");
+  *n_out = 0;
+  if (n == 0) return ILC_OK;
+  if (!xyz || !center || !extent || !periodic || !out_xyzq)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid ingest arguments");
+  if (n >= (1ull << 32)) return fail(c, ILC_ERR_INVALID_ARGUMENT, "at most 2^32 - 1 cells");
+  CutoutParams p;
+  for (int j = 0; j < 3; ++j) {
+    if (!std::isfinite(center[j]) || !(extent[j] >= 0.0) || !std::isfinite(extent[j]) ||
+        !(periodic[j] >= 0.0) || !std::isfinite(periodic[j]))
+      return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid cutout center, extent or period");
+    // volume_cutout bounding box and the border-widened box of correct_periodicity
+    p.lo[j] = center[j] - 0.5 * extent[j];
+    p.hi[j] = center[j] + 0.5 * extent[j];
+    p.glo[j] = p.lo[j] - border;
+    p.ghi[j] = p.hi[j] + border;
+    p.period[j] = periodic[j];
+  }
+  if (!(border >= 0.0) || !std::isfinite(border))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid border");
+  const void *dx = nullptr, *dq = nullptr;
+  ILC_CUDA(c, stage_in(c, c.in_a, xyz, n * 12, is_device, &dx), "cells H2D");
+  if (q) ILC_CUDA(c, stage_in(c, c.in_b, q, n * 4, is_device, &dq), "quantity H2D");
+  void *dout = nullptr, *didx = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, out_xyzq, n * 16, is_device, &dout), "ingest output");
+  if (out_index) ILC_CUDA(c, out_ptr(c.out_b, out_index, n * 4, is_device, &didx), "index output");
+  ILC_CUDA(c, c.out_c.ensure(64), "count");
+  ILC_CUDA(c, ingest_launch(c, static_cast<const float*>(dx), static_cast<const float*>(dq), n, p,
+                            static_cast<float4*>(dout), static_cast<uint32_t*>(didx),
+                            c.out_c.as<unsigned long long>()),
+           "ingest kernels");
+  unsigned long long kept = 0;
+  ILC_CUDA(c, cudaMemcpyAsync(&kept, c.out_c.p, 8, cudaMemcpyDeviceToHost, c.stream), "count D2H");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "ingest");
+  if (!is_device) {
+    ILC_CUDA(c, cudaMemcpyAsync(out_xyzq, dout, kept * 16, cudaMemcpyDeviceToHost, c.stream),
+             "ingest output D2H");
+    if (out_index)
+      ILC_CUDA(c, cudaMemcpyAsync(out_index, didx, kept * 4, cudaMemcpyDeviceToHost, c.stream),
+               "index output D2H");
+    ILC_CUDA(c, cudaStreamSynchronize(c.stream), "ingest");
+  }
+  *n_out = kept;
+  return ILC_OK;
+}
+
 }  // extern "C"

@@ -277,6 +277,12 @@ cudaError_t grid_bbox(Context& c, const float4* in, uint64_t n, float* mn3, floa
   return cudaSuccess;
 }
 
+cudaError_t exclusive_scan_u32(Context& c, uint32_t* a, uint64_t m) {
+  ++c.launches;
+  scan_kernel<<<1, 1024, 0, c.stream>>>(a, m);
+  return cudaGetLastError();
+}
+
 cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n) {
   cudaError_t e;
   const GridParams& g = c.gp;

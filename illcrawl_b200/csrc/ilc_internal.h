@@ -121,6 +121,20 @@ constexpr size_t kFlagsBytes = 64 + sizeof(DevStats);
 cudaError_t grid_bbox(Context& c, const float4* in, uint64_t n, float* mn3, float* mx3,
                       bool* nonfinite);
 cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n);
+// In-place exclusive prefix sum of m uint32 (one block; for per-block counts).
+cudaError_t exclusive_scan_u32(Context& c, uint32_t* a, uint64_t m);
+
+// Cell ingestion (ilc_ingest.cu): periodic correction and volume cutout of
+// n cells, compacted in input order into (x, y, z, q) float4 and the original
+// indices; *n_out (device uint64) receives the number kept.
+struct CutoutParams {
+  double lo[3], hi[3];     // cutout box: center -/+ extent / 2
+  double glo[3], ghi[3];   // box widened by the border (periodic correction)
+  double period[3];
+};
+cudaError_t ingest_launch(Context& c, const float* xyz, const float* q, uint64_t n,
+                          const CutoutParams& p, float4* out, uint32_t* out_index,
+                          unsigned long long* n_out);
 cudaError_t nn8_query_launch(Context& c, const float4* pts, uint64_t n, bool merge,
                              float* out, int32_t* idx8, float* d8);
 cudaError_t quantity_xray_flux_launch(Context& c, const float* rho, const float* u,

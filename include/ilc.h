@@ -261,6 +261,24 @@ ilc_status ilc_project_xray_flux(ilc_ctx* ctx, const float* cells, const float* 
                                  const ilc_los_scaling* scaling, float* image, int is_device,
                                  ilc_render_stats* stats);
 
+/* ---- cell ingestion ---------------------------------------------------------
+ * The per-row loop of reconstructing_data_crawler::run
+ * (reconstructing_data_crawler.cpp:170-230) on the device: each cell's float
+ * coordinates, widened to double, move by one period along every axis where
+ * that puts them inside the cutout box center -/+ extent/2 widened by border
+ * (coordinate_system::correct_periodicity, coordinate_system.hpp:25-47; the
+ * crawler's border is 100 kpc); cells whose corrected position lies in the
+ * cutout box (volume_cutout::contains_point, reconstructing_data_crawler.cpp:
+ * 49-60) are kept, in input order, as float4 (x, y, z, q) with the corrected
+ * coordinates cast to float, q = their value in q (0 if q is NULL), and their
+ * input index in out_index (may be NULL). xyz: n x 3 floats; out_xyzq: room
+ * for n float4; *n_out: cells kept. The result feeds ilc_nn8_setup_particles
+ * directly. All arrays follow is_device. n < 2^32. */
+ilc_status ilc_ingest_cells(ilc_ctx* ctx, const float* xyz, const float* q, uint64_t n,
+                            const double* center, const double* extent, const double* periodic,
+                            double border, float* out_xyzq, uint32_t* out_index,
+                            uint64_t* n_out, int is_device);
+
 /* ---- batched render ---------------------------------------------------------
  * Many projections in one persistent launch: the (camera, frame) loop of
  * integrated_projection / distributed_animation (animation.cpp:29-100,229-241)

@@ -349,3 +349,24 @@ def ray_span(jb, ix, iy):
     ln = ctypes.c_float(0.0)
     L.orc_ray_span(ctypes.byref(jb), ix, iy, ctypes.byref(m), _p(o), ctypes.byref(ln))
     return bool(m.value), o, ln.value
+
+
+def ingest_cells(xyz, q, center, extent, periodic, border=100.0):
+    """Periodic correction + cutout + compaction of the crawler's row loop:
+    (xyzq (m, 4), input indices (m,))."""
+    L = lib()
+    if not hasattr(L, "_ingest_declared"):
+        P = ctypes.c_void_p
+        L.orc_ingest_cells.argtypes = [P, P, ctypes.c_int64, P, P, P, ctypes.c_double, P, P]
+        L.orc_ingest_cells.restype = ctypes.c_int64
+        L._ingest_declared = True
+    xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    n = xyz.shape[0]
+    qa = None if q is None else np.ascontiguousarray(q, np.float32)
+    out = np.zeros((n, 4), np.float32)
+    idx = np.zeros(n, np.uint32)
+    c3 = lambda v: np.ascontiguousarray(v, np.float64)
+    ce, ex, pe = c3(center), c3(extent), c3(periodic)
+    k = L.orc_ingest_cells(_p(xyz), _p(qa), n, _p(ce), _p(ex), _p(pe), float(border), _p(out),
+                           _p(idx))
+    return out[:k], idx[:k]

@@ -1610,4 +1610,45 @@ int orc_ray_span(const void* job_v, int32_t ix, int32_t iy, int32_t* masked, flo
   return 0;
 }
 
+
+// Cell ingestion of reconstructing_data_crawler::run
+// (reconstructing_data_crawler.cpp:170-230): float coordinates widened to
+// double, coordinate_system::correct_periodicity (coordinate_system.hpp:25-47)
+// against the cutout box widened by `border`, volume_cutout::contains_point
+// with zero tolerance (reconstructing_data_crawler.cpp:49-60), kept cells in
+// input order with the corrected coordinates cast to float
+// (to_device_vector4, cl_types.hpp:55-61). Returns the number kept.
+int64_t orc_ingest_cells(const float* xyz, const float* q, int64_t n, const double* center,
+                         const double* extent, const double* periodic, double border,
+                         float* out_xyzq, uint32_t* out_index) {
+  double bmin[3], bmax[3];
+  for (int j = 0; j < 3; ++j) {
+    bmin[j] = center[j] - 0.5 * extent[j];  // get_bounding_box_min_corner
+    bmax[j] = center[j] + 0.5 * extent[j];
+  }
+  int64_t k = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double c[3];
+    for (int j = 0; j < 3; ++j) c[j] = (double)xyz[3 * i + j];
+    for (int j = 0; j < 3; ++j) {
+      const double gmin = bmin[j] - border, gmax = bmax[j] + border;
+      if (gmin <= c[j] - periodic[j] && c[j] - periodic[j] <= gmax)
+        c[j] -= periodic[j];
+      else if (gmin <= c[j] + periodic[j] && c[j] + periodic[j] <= gmax)
+        c[j] += periodic[j];
+    }
+    bool in = true;
+    for (int j = 0; j < 3; ++j) {
+      if (c[j] < (center[j] - 0.5 * extent[j] - 0.0)) in = false;
+      if (c[j] > (center[j] + 0.5 * extent[j] + 0.0)) in = false;
+    }
+    if (!in) continue;
+    for (int j = 0; j < 3; ++j) out_xyzq[4 * k + j] = (float)c[j];
+    out_xyzq[4 * k + 3] = q ? q[i] : 0.0f;
+    if (out_index) out_index[k] = (uint32_t)i;
+    ++k;
+  }
+  return k;
+}
+
 }  // extern "C"
