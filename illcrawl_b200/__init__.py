@@ -331,6 +331,13 @@ class Context:
             _ptr(g_r), _ptr(g_t), 0, ctypes.byref(st)))
         return img, g_r, g_t, st.as_dict()
 
+    # ---- volumetric slice
+    def volumetric_slice(self, cam, dV=1.0, additional_samples=0, seed=0):
+        img = self._image(cam, False)
+        self.check(self.L.ilc_volumetric_slice(self.h, ctypes.byref(cam), float(dV),
+                                               int(additional_samples), int(seed), _ptr(img), 0))
+        return img
+
     # ---- cell ingestion
     def ingest_cells(self, xyz, q, center, extent, periodic, border=100.0):
         """Periodic correction + cutout + compaction (ilc_ingest_cells). Host

@@ -1192,4 +1192,27 @@ ilc_status ilc_ingest_cells(ilc_ctx* h, const float* xyz, const float* q, uint64
   return ILC_OK;
 }
 
+
+ilc_status ilc_volumetric_slice(ilc_ctx* h, const ilc_camera* cam, double dV,
+                                int32_t additional_samples, uint64_t seed, float* image,
+                                int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "slice before setup_particles");
+  if (!camera_ok(cam) || !image || additional_samples < 0 || !std::isfinite(dV))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid slice arguments");
+  float f[13];
+  double d[13];
+  camera_plane(*cam, f, d);
+  const uint64_t npix = (uint64_t)cam->num_pix_x * (uint64_t)cam->num_pix_y;
+  void* dimg = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, image, npix * 4, is_device, &dimg), "slice image");
+  ILC_CUDA(c, slice_launch(c, d, cam->num_pix_x, cam->num_pix_y, additional_samples + 1, seed, dV,
+                           static_cast<float*>(dimg)),
+           "slice kernels");
+  ILC_CUDA(c, finish_out(c, image, dimg, npix * 4, is_device), "slice");
+  return ILC_OK;
+}
+
 }  // extern "C"

@@ -132,6 +132,10 @@ struct CutoutParams {
   double glo[3], ghi[3];   // box widened by the border (periodic correction)
   double period[3];
 };
+// volumetric_slice::create_slice (ilc_slice.cu); plane = camera_plane's double
+// output (look, basis0, basis1, min corner, pixel size); out: device image.
+cudaError_t slice_launch(Context& c, const double plane[13], int nx, int ny, int samples,
+                         uint64_t seed, double dV, float* out);
 cudaError_t ingest_launch(Context& c, const float* xyz, const float* q, uint64_t n,
                           const CutoutParams& p, float4* out, uint32_t* out_index,
                           unsigned long long* n_out);

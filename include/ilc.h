@@ -261,6 +261,21 @@ ilc_status ilc_project_xray_flux(ilc_ctx* ctx, const float* cells, const float* 
                                  const ilc_los_scaling* scaling, float* image, int is_device,
                                  ilc_render_stats* stats);
 
+/* ---- volumetric slice ---------------------------------------------------------
+ * volumetric_slice::create_slice (volumetric_slice.cpp:31-101): the nn8
+ * reconstruction of the particles' q at every pixel of the camera plane,
+ * sample 0 at camera::get_pixel_coordinate(x, y) (camera.cpp:49-54),
+ * image[y][x] accumulated as the reference does (float pixel += dV * value /
+ * samples, each increment in double). dV is the quantity's
+ * effective_volume_integration_dV (quantity.hpp:193-197,477-480).
+ * additional_samples > 0 adds jittered samples per pixel; the reference
+ * draws their offsets from std::random_device, here they come from a hash of
+ * (seed, sample, pixel), so a slice is reproducible. image: num_pix_y x
+ * num_pix_x floats. */
+ilc_status ilc_volumetric_slice(ilc_ctx* ctx, const ilc_camera* cam, double dV,
+                                int32_t additional_samples, uint64_t seed, float* image,
+                                int is_device);
+
 /* ---- cell ingestion ---------------------------------------------------------
  * The per-row loop of reconstructing_data_crawler::run
  * (reconstructing_data_crawler.cpp:170-230) on the device: each cell's float

@@ -370,3 +370,14 @@ def ingest_cells(xyz, q, center, extent, periodic, border=100.0):
     k = L.orc_ingest_cells(_p(xyz), _p(qa), n, _p(ce), _p(ex), _p(pe), float(border), _p(out),
                            _p(idx))
     return out[:k], idx[:k]
+
+
+def volumetric_slice(grid, cam, dV=1.0, nthreads=0):
+    L = lib()
+    if not hasattr(L, "_slice_declared"):
+        P = ctypes.c_void_p
+        L.orc_volumetric_slice.argtypes = [P, P, ctypes.c_double, P, ctypes.c_int]
+        L._slice_declared = True
+    out = np.zeros(cam.nx * cam.ny, np.float32)
+    L.orc_volumetric_slice(grid.h, ctypes.byref(cam), float(dV), _p(out), nthreads)
+    return out.reshape(cam.ny, cam.nx)

@@ -1651,4 +1651,29 @@ int64_t orc_ingest_cells(const float* xyz, const float* q, int64_t n, const doub
   return k;
 }
 
+
+// volumetric_slice::create_slice (volumetric_slice.cpp:31-101) with no extra
+// samples: nn8 value at camera::get_pixel_coordinate(x, y) (camera.cpp:49-54,
+// double, cast to float), output = 0 + dV * value / 1 in double, cast to float.
+int orc_volumetric_slice(void* h, const orc_camera* c, double dV, float* out, int nthreads) {
+  Grid* g = (Grid*)h;
+  Camera cam;
+  std::memcpy(&cam, c, sizeof(Camera));
+  CamDev d;
+  camera_setup(cam, &d);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const int64_t npix = (int64_t)cam.nx * cam.ny;
+#pragma omp parallel for schedule(static)
+  for (int64_t p = 0; p < npix; ++p) {
+    const double xs = (double)(p % cam.nx), ys = (double)(p / cam.nx);
+    float q[3];
+    for (int j = 0; j < 3; ++j)
+      q[j] = (float)((d.minp_d[j] + xs * d.ps_d * d.b0_d[j]) + ys * d.ps_d * d.b1_d[j]);
+    const float v = nn8_value<float>(*g, q[0], q[1], q[2], nullptr);
+    const float acc = 0.0f;
+    out[p] = (float)((double)acc + dV * (double)v / 1.0);
+  }
+  return 0;
+}
+
 }  // extern "C"
