@@ -338,6 +338,13 @@ class Context:
                                                int(additional_samples), int(seed), _ptr(img), 0))
         return img
 
+    def volumetric_tomography(self, cam, dV=1.0, initial_z_step=0, num_steps=1):
+        cube = np.zeros((num_steps, cam.num_pix_y, cam.num_pix_x), np.float32)
+        self.check(self.L.ilc_volumetric_tomography(self.h, ctypes.byref(cam), float(dV),
+                                                    int(initial_z_step), int(num_steps),
+                                                    _ptr(cube), 0))
+        return cube
+
     # ---- cell ingestion
     def ingest_cells(self, xyz, q, center, extent, periodic, border=100.0):
         """Periodic correction + cutout + compaction (ilc_ingest_cells). Host

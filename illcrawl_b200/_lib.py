@@ -118,6 +118,7 @@ SIGNATURES = {
     "ilc_quantity_xray_spectrum": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _P, _P, _i32, _P,
                                           _int]),
     "ilc_volumetric_slice": (_int, [_P, _P, _f64, _i32, _u64, _P, _int]),
+    "ilc_volumetric_tomography": (_int, [_P, _P, _f64, _i64, _i64, _P, _int]),
     "ilc_ingest_cells": (_int, [_P, _P, _P, _u64, _P, _P, _P, _f64, _P, _P, _P, _int]),
     "ilc_render_batched": (_int, [_P, _P, _i32, _int, _P, _i32, Tolerance, _P, _u64, _int, _P]),
     "ilc_set_batch_schedule": (_int, [_P, _i32, _i32, _f32, _i32]),

@@ -1215,4 +1215,36 @@ ilc_status ilc_volumetric_slice(ilc_ctx* h, const ilc_camera* cam, double dV,
   return ILC_OK;
 }
 
+
+ilc_status ilc_volumetric_tomography(ilc_ctx* h, const ilc_camera* cam, double dV,
+                                     int64_t initial_z_step, int64_t num_steps, float* cube,
+                                     int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "tomography before setup_particles");
+  if (!camera_ok(cam) || !cube || initial_z_step < 0 || num_steps < 0 || !std::isfinite(dV))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid tomography arguments");
+  if (num_steps == 0) return ILC_OK;
+  const uint64_t npix = (uint64_t)cam->num_pix_x * (uint64_t)cam->num_pix_y;
+  void* dcube = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, cube, npix * (uint64_t)num_steps * 4, is_device, &dcube),
+           "tomography cube");
+  const double ps = cam->screen_width / (double)cam->num_pix_x;
+  for (int64_t z = 0; z < num_steps; ++z) {
+    // camera moved along look_at by (initial + z) pixel sizes (volumetric_tomography.cpp:81-82)
+    ilc_camera mc = *cam;
+    const double t = (double)(initial_z_step + z) * ps;
+    for (int j = 0; j < 3; ++j) mc.position[j] = cam->position[j] + t * cam->look_at[j];
+    float f[13];
+    double d[13];
+    camera_plane(mc, f, d);
+    ILC_CUDA(c, slice_launch(c, d, cam->num_pix_x, cam->num_pix_y, 1, 0, dV,
+                             static_cast<float*>(dcube) + (uint64_t)z * npix),
+             "tomography slice");
+  }
+  ILC_CUDA(c, finish_out(c, cube, dcube, npix * (uint64_t)num_steps * 4, is_device), "tomography");
+  return ILC_OK;
+}
+
 }  // extern "C"

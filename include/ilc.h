@@ -276,6 +276,15 @@ ilc_status ilc_volumetric_slice(ilc_ctx* ctx, const ilc_camera* cam, double dV,
                                 int32_t additional_samples, uint64_t seed, float* image,
                                 int is_device);
 
+/* volumetric_tomography::create_tomographic_cube (volumetric_tomography.cpp:
+ * 62-101): num_steps slices of ilc_volumetric_slice (one sample per pixel),
+ * slice z taken with the camera moved along look_at by (initial_z_step + z)
+ * pixel sizes. cube: num_steps x num_pix_y x num_pix_x floats (x fastest, as
+ * the reference's cube). */
+ilc_status ilc_volumetric_tomography(ilc_ctx* ctx, const ilc_camera* cam, double dV,
+                                     int64_t initial_z_step, int64_t num_steps, float* cube,
+                                     int is_device);
+
 /* ---- cell ingestion ---------------------------------------------------------
  * The per-row loop of reconstructing_data_crawler::run
  * (reconstructing_data_crawler.cpp:170-230) on the device: each cell's float
