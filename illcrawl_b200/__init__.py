@@ -90,6 +90,39 @@ def pack_jobs(jobs, n_channels):
     return arr, off
 
 
+def write_fits(path, data, cards=()):
+    """FITS image / cube of float32 data (ilc_fits_write_image). data: (ny, nx)
+    or (nz, ny, nx). cards: (key, value[, comment]) with float, int, bool or
+    str values, appended as the reference appends its settings."""
+    a = np.ascontiguousarray(data, np.float32)
+    if a.ndim not in (2, 3):
+        raise ValueError("2 or 3 dimensions")
+    naxes = np.ascontiguousarray(a.shape[::-1], np.int64)
+    arr = (_lib.FitsCard * max(1, len(cards)))()
+    keep = []
+    for i, c in enumerate(cards):
+        key, val = c[0], c[1]
+        com = c[2] if len(c) > 2 else None
+        k = _lib.FitsCard()
+        k.key = key.encode()
+        keep.append(k.key)
+        if isinstance(val, bool):
+            k.type, k.integer = 3, int(val)
+        elif isinstance(val, (int, np.integer)):
+            k.type, k.integer = 1, int(val)
+        elif isinstance(val, (float, np.floating)):
+            k.type, k.number = 0, float(val)
+        else:
+            k.type, k.text = 2, str(val).encode()
+        k.comment = None if com is None else com.encode()
+        arr[i] = k
+    L = _lib.load()
+    st = L.ilc_fits_write_image(str(path).encode(), _ptr(a), a.ndim, _ptr(naxes), arr,
+                                len(cards))
+    if st:
+        raise IlcError(st, f"could not write {path}")
+
+
 def camera_plane(cam):
     out = np.zeros(13, np.float32)
     st = _lib.load().ilc_camera_plane(ctypes.byref(cam), _ptr(out))

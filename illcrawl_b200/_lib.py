@@ -71,6 +71,12 @@ class AdjointStats(ctypes.Structure):
 ADJOINT_CHECKPOINT, ADJOINT_RECOMPUTE = 0, 1
 
 
+class FitsCard(ctypes.Structure):
+    _fields_ = [("key", ctypes.c_char_p), ("type", ctypes.c_int32), ("number", ctypes.c_double),
+                ("integer", ctypes.c_int64), ("text", ctypes.c_char_p),
+                ("comment", ctypes.c_char_p)]
+
+
 class Job(ctypes.Structure):
     """ilc_job: one camera of a batched render."""
     _fields_ = [("camera", Camera), ("z_range", ctypes.c_double),
@@ -119,6 +125,7 @@ SIGNATURES = {
                                           _int]),
     "ilc_volumetric_slice": (_int, [_P, _P, _f64, _i32, _u64, _P, _int]),
     "ilc_volumetric_tomography": (_int, [_P, _P, _f64, _i64, _i64, _P, _int]),
+    "ilc_fits_write_image": (_int, [ctypes.c_char_p, _P, _i32, _P, _P, _i32]),
     "ilc_ingest_cells": (_int, [_P, _P, _P, _u64, _P, _P, _P, _f64, _P, _P, _P, _int]),
     "ilc_render_batched": (_int, [_P, _P, _i32, _int, _P, _i32, Tolerance, _P, _u64, _int, _P]),
     "ilc_set_batch_schedule": (_int, [_P, _i32, _i32, _f32, _i32]),

@@ -303,6 +303,27 @@ ilc_status ilc_ingest_cells(ilc_ctx* ctx, const float* xyz, const float* q, uint
                             double border, float* out_xyzq, uint32_t* out_index,
                             uint64_t* n_out, int is_device);
 
+/* ---- FITS output --------------------------------------------------------------
+ * Writes an image (naxis = 2) or cube (naxis = 3; NAXIS1 = x fastest, as the
+ * renders and ilc_render_batched's per-job blocks are laid out) of floats as a
+ * FITS primary HDU with BITPIX = -32, the structure util::fits::save
+ * (fits.hpp:215-258) produces through cfitsio, followed by header keys as
+ * util::fits_header::add_entry (fits.hpp:142-200) appends them (a COMMENT card
+ * with the key's comment, then the key; keys longer than 8 characters as
+ * HIERARCH cards). Host memory only; no GPU needed. */
+enum { ILC_FITS_DOUBLE = 0, ILC_FITS_INTEGER = 1, ILC_FITS_STRING = 2, ILC_FITS_LOGICAL = 3 };
+typedef struct ilc_fits_card {
+  const char* key;
+  int32_t type;           /* ILC_FITS_* */
+  double number;          /* DOUBLE */
+  int64_t integer;        /* INTEGER, LOGICAL (0 / 1) */
+  const char* text;       /* STRING */
+  const char* comment;    /* may be NULL */
+} ilc_fits_card;
+ilc_status ilc_fits_write_image(const char* path, const float* data, int32_t naxis,
+                                const int64_t* naxes, const ilc_fits_card* cards,
+                                int32_t n_cards);
+
 /* ---- batched render ---------------------------------------------------------
  * Many projections in one persistent launch: the (camera, frame) loop of
  * integrated_projection / distributed_animation (animation.cpp:29-100,229-241)
