@@ -61,3 +61,43 @@ def test_create_without_device_fails_loudly(cuda_lib):
 def test_gaunt_loader_matches_numpy(gaunt_table):
     t = np.loadtxt(os.path.join(ROOT, "illcrawl_b200", "data", "gaunt_factor.dat"), np.float32)
     assert np.array_equal(gaunt_table, t)
+
+
+def test_every_entry_point_rejects_a_null_context(cuda_lib):
+    """With no context (ilc_create returns NULL without a GPU) every entry point
+    returns an error status, a zero count or an error string -- never crashes."""
+    from illcrawl_b200 import _lib
+    L = _lib.load()
+    skip = {"ilc_create", "ilc_destroy", "ilc_camera_plane", "ilc_los_scale",
+            "ilc_grid_build_noalloc", "ilc_fits_write_image"}  # context-free by design
+    checked = 0
+    for name, (res, args) in _lib.SIGNATURES.items():
+        if name in skip:
+            continue
+        fn = getattr(L, name)
+        vals = []
+        for a in args:
+            if a is _lib.Tolerance:
+                vals.append(_lib.Tolerance(0.0, 1e-3))
+            elif a in (ctypes.c_float, ctypes.c_double):
+                vals.append(1.0)
+            elif a is ctypes.c_char_p:
+                vals.append(b"")
+            elif a is ctypes.c_void_p:
+                vals.append(None)
+            else:
+                vals.append(1)
+        r = fn(*vals)
+        if name == "ilc_last_error":
+            assert r == b"null context"
+        elif name in ("ilc_kernel_launches",):
+            assert r == 0
+        elif name == "ilc_get_stream":
+            assert r is None
+        else:
+            assert r == 1, (name, r)  # ILC_ERR_INVALID_ARGUMENT
+        checked += 1
+    assert checked >= 25
+    # the context-free entry points reject bad arguments too
+    assert L.ilc_fits_write_image(None, None, 2, None, None, 0) == 1
+    assert L.ilc_grid_build_noalloc(None, 0, None, None, 0, None, None, None) == 1
