@@ -119,6 +119,78 @@ inline ilc_render_stats create_projection(context& ctx, const ilc_camera& cam, d
   return st;
 }
 
+// The crawler's per-row loop (reconstructing_data_crawler.cpp:170-230): cells
+// (x, y, z triples) periodically corrected and cut to the volume, kept cells in
+// input order as particles with their q.
+inline std::vector<particle> ingest_cells(context& ctx, const std::vector<float>& xyz,
+                                          const std::vector<float>& q, const double center[3],
+                                          const double extent[3], const double periodic[3],
+                                          double border = 100.0,
+                                          std::vector<uint32_t>* index = nullptr) {
+  const uint64_t n = xyz.size() / 3;
+  std::vector<particle> out(n);
+  std::vector<uint32_t> idx(n);
+  uint64_t kept = 0;
+  ctx.check(ilc_ingest_cells(ctx.get(), xyz.data(), q.empty() ? nullptr : q.data(), n, center,
+                             extent, periodic, border, reinterpret_cast<float*>(out.data()),
+                             idx.data(), &kept, 0));
+  out.resize(kept);
+  if (index) {
+    idx.resize(kept);
+    *index = std::move(idx);
+  }
+  return out;
+}
+
+// spectrum_generator / multi_quantity_integrated_projection
+// (spectrum.hpp:81-126, animation.cpp:264-283) for X-ray spectra: the per-cell
+// bin table and one batched render of every camera. The particles (cell
+// positions) must be set up; rho, u, xe are the cells' fields in that order.
+// cube: per camera, n_bins slices of num_pix_y x num_pix_x.
+inline ilc_render_stats render_xray_spectra(context& ctx, const std::vector<float>& rho,
+                                            const std::vector<float>& u,
+                                            const std::vector<float>& xe, float redshift,
+                                            float luminosity_distance,
+                                            const std::vector<float>& energies,
+                                            const std::vector<float>& widths,
+                                            std::vector<ilc_job>& jobs, double rel_tol,
+                                            std::vector<float>& cube) {
+  const uint64_t n = rho.size();
+  const int32_t nb = (int32_t)energies.size();
+  std::vector<float> table(n * (uint64_t)nb);
+  ctx.check(ilc_quantity_xray_spectrum(ctx.get(), rho.data(), u.data(), xe.data(), n, redshift,
+                                       luminosity_distance, energies.data(), widths.data(), nb,
+                                       table.data(), 0));
+  uint64_t off = 0;
+  for (auto& j : jobs) {
+    j.out_offset = off;
+    off += (uint64_t)nb * (uint64_t)j.camera.num_pix_x * (uint64_t)j.camera.num_pix_y;
+  }
+  cube.assign(off, 0.0f);
+  ilc_render_stats st{};
+  ctx.check(ilc_render_batched(ctx.get(), table.data(), nb, 0, jobs.data(), (int32_t)jobs.size(),
+                               ilc_tolerance{0.0, rel_tol}, cube.data(), off, 0, &st));
+  return st;
+}
+
+// volumetric_slice::create_slice (volumetric_slice.cpp:31-101), one sample per
+// pixel unless additional_samples > 0; image is num_pix_y x num_pix_x.
+inline void volumetric_slice(context& ctx, const ilc_camera& cam, double dV,
+                             std::vector<float>& image, int additional_samples = 0,
+                             uint64_t seed = 0) {
+  image.assign((std::size_t)cam.num_pix_x * (std::size_t)cam.num_pix_y, 0.0f);
+  ctx.check(ilc_volumetric_slice(ctx.get(), &cam, dV, additional_samples, seed, image.data(), 0));
+}
+
+// util::fits<float>::save + fits_header::add_entry (fits.hpp:142-258).
+inline void write_fits(const std::string& path, const std::vector<float>& data,
+                       const std::vector<int64_t>& naxes,
+                       const std::vector<ilc_fits_card>& cards = {}) {
+  const ilc_status st = ilc_fits_write_image(path.c_str(), data.data(), (int32_t)naxes.size(),
+                                             naxes.data(), cards.data(), (int32_t)cards.size());
+  if (st != ILC_OK) throw error(st, "could not write " + path);
+}
+
 }  // namespace ilc
 
 #endif  // ILC_BACKEND_HPP
