@@ -40,7 +40,7 @@ int main() {
     }
     const double centre[3] = {50, 50, 50}, extent[3] = {80, 80, 80}, period[3] = {100, 100, 100};
     std::vector<uint32_t> kept_index;
-    auto kept = ilc::ingest_cells(ctx, xyz, q, centre, extent, period, 100.0, &kept_index);
+    auto kept = ilc::ingest_cells(ctx, xyz, q, centre, extent, period, 5.0, &kept_index);
     backend.setup_particles(kept);
     std::vector<float> slice;
     ilc::volumetric_slice(ctx, cam, 1.0, slice);
