@@ -80,3 +80,26 @@ def test_joint_steps_within_tolerance_of_fp64_per_channel(oracle_mod):
     # the same bar as the plain adaptive render: 2x rtol for the bulk (the
     # RKF controls the local error per step, not the per-pixel total)
     assert np.median(rel) < 2e-3 and np.quantile(rel, 0.9) < 2e-3 and rel.max() < 1e-2
+
+
+def test_empty_chords_and_full_masks_give_zero(oracle_mod):
+    c, pts, g = _grid(oracle_mod, n=5_000, seed=44)
+    # camera looking away from the sphere: every chord starts behind the plane
+    cam = oracle_mod.camera((500, 500, 2000), (0, 0, 1), 0.0, 400.0, 6, 5)
+    jb = oracle_mod.job(cam, sphere_center=(500, 500, 500), sphere_radius=300.0, min_chord=0.0)
+    out, st, rc = oracle_mod.render_batched(g, c.rho, [jb])
+    assert rc == 0 and np.all(out == 0.0) and st[0] == 0
+    # an aperture smaller than half a pixel masks every pixel
+    cam2 = oracle_mod.camera((500, 500, 0), (0, 0, 1), 0.0, 400.0, 6, 6)
+    jb2 = oracle_mod.job(cam2, z_range=1000.0, aperture_radius=1e-3)
+    out, st, rc = oracle_mod.render_batched(g, np.stack([c.rho] * 3, 1), [jb2])
+    assert rc == 0 and np.all(out == 0.0) and st[0] == 0
+
+
+def test_scale_multiplies_every_channel(oracle_mod):
+    c, pts, g = _grid(oracle_mod, n=5_000, seed=45)
+    cam = oracle_mod.camera((500, 500, 0), (0, 0, 1), 0.0, 600.0, 5, 4)
+    v = np.stack([c.rho, 2 * c.rho], 1).astype(np.float32)
+    a, _, _ = oracle_mod.render_batched(g, v, [oracle_mod.job(cam, z_range=1000.0, scale=1.0)])
+    b, _, _ = oracle_mod.render_batched(g, v, [oracle_mod.job(cam, z_range=1000.0, scale=0.25)])
+    assert np.array_equal(b, (a * np.float32(0.25)).astype(np.float32))
