@@ -7,8 +7,9 @@ benchmark. Names follow the reference's interfaces:
   (reconstruction_backend.hpp:35-58, volumetric_reconstruction_backend_nn8.hpp:36-82)
 * :func:`create_projection` -- ``volumetric_integration::create_projection``
   (volumetric_integration.cpp:32-88)
-* :func:`xray_flux`, :func:`xray_spectral_flux`, :func:`mean_temperature` -- the
-  quantity kernels of quantities.cl
+* :func:`xray_flux`, :func:`xray_spectral_flux`, :func:`xray_photon_flux`,
+  :func:`chandra_count_rate`, :func:`chandra_spectral_count_rate`,
+  :func:`mean_temperature` -- the quantity kernels of quantities.cl
 * :func:`load_gaunt_table` -- ``util::data_table_loader`` on gaunt_factor.dat
   (data_table_loader.hpp:39-97)
 
@@ -295,6 +296,61 @@ class Context:
         self.check(self.L.ilc_quantity_xray_spectrum(self.h, _ptr(rho), _ptr(u), _ptr(xe), n,
                                                      redshift, luminosity_distance, _ptr(e),
                                                      _ptr(w), nb, _ptr(out), dev))
+        return out
+
+    def xray_photon_flux(self, rho, u, xe, redshift=REDSHIFT,
+                         luminosity_distance=LUMINOSITY_DISTANCE, e_min=0.1, e_max=10.0,
+                         num_samples=100):
+        """xray_photon_flux per cell [photons/s/kpc^3/cm^2] (the reference's
+        defaults for the quantity: 0.1-10 keV, 100 samples)."""
+        rho, u, xe, n, out, dev = self._q3(rho, u, xe)
+        self.check(self.L.ilc_quantity_xray_photon_flux(self.h, _ptr(rho), _ptr(u), _ptr(xe), n,
+                                                        redshift, luminosity_distance, e_min,
+                                                        e_max, num_samples, _ptr(out), dev))
+        return out
+
+    def load_arf(self, table, x_min, dx):
+        """Chandra ARF [cm^2]: len(table) samples from x_min [keV] in steps of
+        dx (the caller supplies the table; chandra::arf, chandra.cpp)."""
+        t = np.ascontiguousarray(table, np.float32).ravel()
+        self.check(self.L.ilc_arf_load(self.h, _ptr(t), t.size, x_min, dx))
+        return t
+
+    def chandra_count_rate(self, rho, u, xe, redshift=REDSHIFT,
+                           luminosity_distance=LUMINOSITY_DISTANCE):
+        """Per-cell count rate over every ARF channel [counts/s/kpc^3]."""
+        rho, u, xe, n, out, dev = self._q3(rho, u, xe)
+        self.check(self.L.ilc_quantity_chandra_count_rate(self.h, _ptr(rho), _ptr(u), _ptr(xe),
+                                                          n, redshift, luminosity_distance,
+                                                          _ptr(out), dev))
+        return out
+
+    def chandra_spectral_count_rate(self, rho, u, xe, energy, energy_bin_width,
+                                    redshift=REDSHIFT, luminosity_distance=LUMINOSITY_DISTANCE):
+        """Per-cell count rate in the channel (energy, energy_bin_width)."""
+        rho, u, xe, n, out, dev = self._q3(rho, u, xe)
+        self.check(self.L.ilc_quantity_chandra_spectral_count_rate(
+            self.h, _ptr(rho), _ptr(u), _ptr(xe), n, redshift, luminosity_distance, energy,
+            energy_bin_width, _ptr(out), dev))
+        return out
+
+    def chandra_spectrum(self, rho, u, xe, energies, widths, redshift=REDSHIFT,
+                         luminosity_distance=LUMINOSITY_DISTANCE):
+        """Per-cell count rate in every channel, cell-major (n, n_bins)."""
+        dev = _is_dev(u)
+        if not dev:
+            rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+        e = np.ascontiguousarray(energies, np.float32)
+        w = np.ascontiguousarray(widths, np.float32)
+        n, nb = u.shape[0], e.shape[0]
+        if dev:
+            import torch
+            out = torch.empty((n, nb), dtype=torch.float32, device=u.device)
+        else:
+            out = np.zeros((n, nb), np.float32)
+        self.check(self.L.ilc_quantity_chandra_spectrum(self.h, _ptr(rho), _ptr(u), _ptr(xe), n,
+                                                        redshift, luminosity_distance, _ptr(e),
+                                                        _ptr(w), nb, _ptr(out), dev))
         return out
 
     def mean_temperature(self, u, xe):

@@ -15,6 +15,7 @@ STATUS_NAMES = {
     0: "ILC_OK", 1: "ILC_ERR_INVALID_ARGUMENT", 2: "ILC_ERR_CUDA", 3: "ILC_ERR_OUT_OF_MEMORY",
     4: "ILC_ERR_NO_PARTICLES", 5: "ILC_ERR_NO_GAUNT_TABLE", 6: "ILC_ERR_STEP_LIMIT",
     7: "ILC_ERR_NONFINITE_INPUT", 8: "ILC_ERR_GRID_TOO_LARGE", 9: "ILC_ERR_INTERNAL",
+    10: "ILC_ERR_NO_ARF_TABLE",
 }
 CONTROLLER_REF32 = 0
 CONTROLLER_FP64 = 1
@@ -123,6 +124,14 @@ SIGNATURES = {
     "ilc_set_render_engine": (_int, [_P, _i32]),
     "ilc_quantity_xray_spectrum": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _P, _P, _i32, _P,
                                           _int]),
+    "ilc_quantity_xray_photon_flux": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32,
+                                             _P, _int]),
+    "ilc_arf_load": (_int, [_P, _P, _i32, _f32, _f32]),
+    "ilc_quantity_chandra_count_rate": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _P, _int]),
+    "ilc_quantity_chandra_spectral_count_rate": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _f32,
+                                                        _f32, _P, _int]),
+    "ilc_quantity_chandra_spectrum": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _P, _P, _i32, _P,
+                                             _int]),
     "ilc_volumetric_slice": (_int, [_P, _P, _f64, _i32, _u64, _P, _int]),
     "ilc_volumetric_tomography": (_int, [_P, _P, _f64, _i64, _i64, _P, _int]),
     "ilc_fits_write_image": (_int, [ctypes.c_char_p, _P, _i32, _P, _P, _i32]),

@@ -428,7 +428,7 @@ void ilc_destroy(ilc_ctx* h) {
                     &c.in_b, &c.in_c, &c.out_a, &c.out_b, &c.out_c, &c.spiral, &c.flags,
                     &c.rec_h, &c.rec_n, &c.adj_dT, &c.adj_dR, &c.adj_grad, &c.adj_seed,
                     &c.adj_loss, &c.codes, &c.jobs, &c.chan_sorted, &c.chan_state, &c.queue,
-                    &c.item_cost, &c.item_order})
+                    &c.item_cost, &c.item_order, &c.arf})
     b->release();
   if (c.batch_exec) cudaGraphExecDestroy(c.batch_exec);
   if (c.ev0) cudaEventDestroy(c.ev0);
@@ -642,6 +642,136 @@ ilc_status ilc_quantity_xray_spectral_flux(ilc_ctx* h, const float* rho, const f
                                        energy_bin_width, static_cast<float*>(dout)),
            "xray_spectral_flux kernel");
   ILC_CUDA(c, finish_out(c, out, dout, n * 4, is_device), "xray_spectral_flux");
+  return ILC_OK;
+}
+
+ilc_status ilc_quantity_xray_photon_flux(ilc_ctx* h, const float* rho, const float* u,
+                                         const float* xe, uint64_t n, float redshift,
+                                         float luminosity_distance, float e_min, float e_max,
+                                         int32_t num_samples, float* out, int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (n == 0) return ILC_OK;
+  if (!rho || !u || !xe || !out || num_samples <= 0 || !(e_max >= e_min))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid xray_photon_flux arguments");
+  const float *a, *b, *d;
+  ilc_status st = quantity_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  void* dout = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, out, n * 4, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_xray_photon_flux_launch(c, a, b, d, n, redshift, luminosity_distance,
+                                               e_min, e_max, num_samples,
+                                               static_cast<float*>(dout)),
+           "xray_photon_flux kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, n * 4, is_device), "xray_photon_flux");
+  return ILC_OK;
+}
+
+ilc_status ilc_arf_load(ilc_ctx* h, const float* table, int32_t n, float x_min, float dx) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!table || n <= 0 || n > 65536 || !(dx > 0.0f) || !std::isfinite(dx) ||
+      !std::isfinite(x_min))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid ARF table (1 to 65536 samples, dx > 0)");
+  const size_t bytes = (size_t)n * 4;
+  ILC_CUDA(c, c.arf.ensure(bytes), "arf alloc");
+  ILC_CUDA(c, cudaMemcpyAsync(c.arf.p, table, bytes, cudaMemcpyHostToDevice, c.stream),
+           "arf H2D");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "arf");
+  c.arf_n = n; c.arf_x0 = x_min; c.arf_dx = dx;
+  c.has_arf = true;
+  return ILC_OK;
+}
+
+// Null check and staging of the Chandra quantities' inputs.
+static ilc_status chandra_inputs(Context& c, const float* rho, const float* u, const float* xe,
+                                 uint64_t n, int is_device, const float** a, const float** b,
+                                 const float** d) {
+  if (!rho || !u || !xe) return fail(c, ILC_ERR_INVALID_ARGUMENT, "null input array");
+  return quantity_inputs(c, rho, u, xe, n, is_device, a, b, d);
+}
+
+ilc_status ilc_quantity_chandra_count_rate(ilc_ctx* h, const float* rho, const float* u,
+                                           const float* xe, uint64_t n, float redshift,
+                                           float luminosity_distance, float* out,
+                                           int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (!c.has_arf) return fail(c, ILC_ERR_NO_ARF_TABLE, "ARF table not loaded");
+  if (n == 0) return ILC_OK;
+  if (!out) return fail(c, ILC_ERR_INVALID_ARGUMENT, "null output");
+  const float *a, *b, *d;
+  ilc_status st = chandra_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  void* dout = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, out, n * 4, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_chandra_total_launch(c, a, b, d, n, redshift, luminosity_distance,
+                                            static_cast<float*>(dout)),
+           "chandra_count_rate kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, n * 4, is_device), "chandra_count_rate");
+  return ILC_OK;
+}
+
+ilc_status ilc_quantity_chandra_spectral_count_rate(ilc_ctx* h, const float* rho,
+                                                    const float* u, const float* xe,
+                                                    uint64_t n, float redshift,
+                                                    float luminosity_distance, float energy,
+                                                    float energy_bin_width, float* out,
+                                                    int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (!c.has_arf) return fail(c, ILC_ERR_NO_ARF_TABLE, "ARF table not loaded");
+  if (n == 0) return ILC_OK;
+  if (!out) return fail(c, ILC_ERR_INVALID_ARGUMENT, "null output");
+  const float *a, *b, *d;
+  ilc_status st = chandra_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  void* dout = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_a, out, n * 4, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_chandra_bin_launch(c, a, b, d, n, redshift, luminosity_distance, energy,
+                                          energy_bin_width, static_cast<float*>(dout)),
+           "chandra_spectral_count_rate kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, n * 4, is_device), "chandra_spectral_count_rate");
+  return ILC_OK;
+}
+
+ilc_status ilc_quantity_chandra_spectrum(ilc_ctx* h, const float* rho, const float* u,
+                                         const float* xe, uint64_t n, float redshift,
+                                         float luminosity_distance, const float* energies,
+                                         const float* widths, int32_t n_bins, float* out,
+                                         int is_device) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_gaunt) return fail(c, ILC_ERR_NO_GAUNT_TABLE, "Gaunt table not loaded");
+  if (!c.has_arf) return fail(c, ILC_ERR_NO_ARF_TABLE, "ARF table not loaded");
+  if (n == 0) return ILC_OK;
+  if (!out || !energies || !widths || n_bins < 1)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid chandra_spectrum arguments");
+  const float *a, *b, *d;
+  ilc_status st = chandra_inputs(c, rho, u, xe, n, is_device, &a, &b, &d);
+  if (st) return st;
+  std::vector<float> ed(2 * (size_t)n_bins);
+  std::memcpy(ed.data(), energies, 4 * (size_t)n_bins);
+  std::memcpy(ed.data() + n_bins, widths, 4 * (size_t)n_bins);
+  ILC_CUDA(c, c.out_c.ensure(8 * (size_t)n_bins), "bin table");
+  ILC_CUDA(c, cudaMemcpyAsync(c.out_c.p, ed.data(), 8 * (size_t)n_bins, cudaMemcpyHostToDevice,
+                              c.stream), "bin table H2D");
+  void* dout = nullptr;
+  const size_t bytes = n * (size_t)n_bins * 4;
+  ILC_CUDA(c, out_ptr(c.out_a, out, bytes, is_device, &dout), "out");
+  ILC_CUDA(c, quantity_chandra_bins_launch(c, a, b, d, n, redshift, luminosity_distance,
+                                           c.out_c.as<float>(), c.out_c.as<float>() + n_bins,
+                                           n_bins, static_cast<float*>(dout)),
+           "chandra_spectrum kernel");
+  ILC_CUDA(c, finish_out(c, out, dout, bytes, is_device), "chandra_spectrum");
   return ILC_OK;
 }
 

@@ -72,6 +72,12 @@ struct Context {
   int32_t gw = 0, gh = 0;
   float gx0 = 0, gy0 = 0, gdx = 0, gdy = 0;
 
+  // Chandra ARF (1D tabulated function)
+  bool has_arf = false;
+  DevBuf arf;
+  int32_t arf_n = 0;
+  float arf_x0 = 0, arf_dx = 0;
+
   // nn8 running lists for multi-block merging (volumetric_reconstruction_backend_nn8.cpp:57-66)
   DevBuf list_d, list_v, list_id;
   uint64_t list_n = 0;
@@ -153,6 +159,20 @@ cudaError_t quantity_xray_bins_launch(Context& c, const float* rho, const float*
                                       const float* e, const float* de, int n_bins, float* out);
 cudaError_t quantity_temperature_launch(Context& c, const float* u, const float* xe,
                                         uint64_t n, float* out);
+cudaError_t quantity_xray_photon_flux_launch(Context& c, const float* rho, const float* u,
+                                             const float* xe, uint64_t n, float z, float dL,
+                                             float emin, float emax, int num_samples,
+                                             float* out);
+cudaError_t quantity_chandra_total_launch(Context& c, const float* rho, const float* u,
+                                          const float* xe, uint64_t n, float z, float dL,
+                                          float* out);
+cudaError_t quantity_chandra_bin_launch(Context& c, const float* rho, const float* u,
+                                        const float* xe, uint64_t n, float z, float dL, float e,
+                                        float de, float* out);
+cudaError_t quantity_chandra_bins_launch(Context& c, const float* rho, const float* u,
+                                         const float* xe, uint64_t n, float z, float dL,
+                                         const float* e, const float* de, int n_bins,
+                                         float* out);
 
 struct RenderArgs {
   float cam[13];        // look(3), b0(3), b1(3), min corner(3), pixel size

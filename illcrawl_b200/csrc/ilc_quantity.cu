@@ -1,6 +1,8 @@
 // ilc_quantity.cu -- per-cell quantity transforms of the X-ray path
-// (quantities.cl:38-136, 156-239, 354-430) with the thermally averaged Gaunt
-// factor table (gaunt_factor.cpp:30-41) resident in shared memory.
+// (quantities.cl:38-136, 156-260, 354-675) with the thermally averaged Gaunt
+// factor table (gaunt_factor.cpp:30-41) resident in shared memory and the
+// Chandra ARF (chandra.cpp, class chandra::arf) read through the read-only
+// cache.
 //
 // The OpenCL image lookup (read_imagef, CLK_FILTER_LINEAR, CLK_ADDRESS_CLAMP,
 // unnormalised coordinates; tabulated_function.cl:26-59) is done in software
@@ -19,7 +21,10 @@ __device__ __forceinline__ void load_table(float* dst, const float* __restrict__
   __syncthreads();
 }
 
-// xray_flux (quantities.cl:354-385)
+// xray_flux (quantities.cl:354-385); kPhoton: xray_photon_flux
+// (quantities.cl:640-675), the band integral of emission / photon energy,
+// converted from per m^2 to per cm^2.
+template <bool kPhoton>
 __global__ void __launch_bounds__(256)
 xray_flux_kernel(const float* __restrict__ table, GauntView G, const float* __restrict__ rho,
                  const float* __restrict__ u, const float* __restrict__ xe, uint64_t n, float z,
@@ -30,8 +35,69 @@ xray_flux_kernel(const float* __restrict__ table, GauntView G, const float* __re
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const float T = temperature(u[i], xe[i]);
-    out[i * stride] = band_flux(t, G, (1.f + z) * emin, (1.f + z) * emax,
-                                1.f / (float)num_samples, T, xe[i], rho[i], dL);
+    const float f = band_flux<kPhoton>(t, G, (1.f + z) * emin, (1.f + z) * emax,
+                                       1.f / (float)num_samples, T, xe[i], rho[i], dL);
+    out[i * stride] = kPhoton ? f * 1.e-4f : f;
+  }
+}
+
+// chandra_xray_total_count_rate (quantities.cl:510-557): the count rate summed
+// in channel order over every ARF channel k, at energy x0 + k * dx with
+// width dx. The channel energy is the same for all threads of a warp, so the
+// ARF reads are broadcasts.
+__global__ void __launch_bounds__(256)
+chandra_total_kernel(const float* __restrict__ table, GauntView G, const float* __restrict__ arf,
+                     ArfView A, const float* __restrict__ rho, const float* __restrict__ u,
+                     const float* __restrict__ xe, uint64_t n, float z, float dL,
+                     float* __restrict__ out) {
+  __shared__ float t[kMaxTable];
+  load_table(t, table, G.w * G.h);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float T = temperature(u[i], xe[i]);
+    const float x = xe[i], r = rho[i];
+    float em = 0.0f;
+    for (int k = 0; k < A.n; ++k) {
+      const float e = A.x0 + (float)k * A.dx;
+      em += chandra_rate(t, G, arf, A, e, A.dx, z, T, x, r, dL);
+    }
+    out[i] = em;
+  }
+}
+
+// chandra_xray_spectral_count_rate (quantities.cl:584-622): one channel.
+__global__ void __launch_bounds__(256)
+chandra_bin_kernel(const float* __restrict__ table, GauntView G, const float* __restrict__ arf,
+                   ArfView A, const float* __restrict__ rho, const float* __restrict__ u,
+                   const float* __restrict__ xe, uint64_t n, float z, float dL, float e,
+                   float de, float* __restrict__ out) {
+  __shared__ float t[kMaxTable];
+  load_table(t, table, G.w * G.h);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float T = temperature(u[i], xe[i]);
+    out[i] = chandra_rate(t, G, arf, A, e, de, z, T, xe[i], rho[i], dL);
+  }
+}
+
+// chandra_xray_spectral_count_rate for n_bins channels at once (the quantity
+// of each frame of chandra_spectrum_quantity_generator, spectrum.cpp:45-65),
+// cell-major out[i * n_bins + b] as ilc_render_batched reads it.
+__global__ void __launch_bounds__(256)
+chandra_bins_kernel(const float* __restrict__ table, GauntView G, const float* __restrict__ arf,
+                    ArfView A, const float* __restrict__ rho, const float* __restrict__ u,
+                    const float* __restrict__ xe, uint64_t n, float z, float dL,
+                    const float* __restrict__ e, const float* __restrict__ de, int n_bins,
+                    float* __restrict__ out) {
+  __shared__ float t[kMaxTable];
+  load_table(t, table, G.w * G.h);
+  const uint64_t total = n * (uint64_t)n_bins;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = k / (uint64_t)n_bins;
+    const int b = (int)(k - i * (uint64_t)n_bins);
+    const float T = temperature(u[i], xe[i]);
+    out[k] = chandra_rate(t, G, arf, A, e[b], de[b], z, T, xe[i], rho[i], dL);
   }
 }
 
@@ -89,8 +155,53 @@ cudaError_t quantity_xray_flux_launch(Context& c, const float* rho, const float*
                                       float emin, float emax, int num_samples, float* out,
                                       int out_stride) {
   GauntView G{c.gw, c.gh, c.gx0, c.gy0, c.gdx, c.gdy};
-  xray_flux_kernel<<<persistent_blocks(n), 256, 0, c.stream>>>(
+  xray_flux_kernel<false><<<persistent_blocks(n), 256, 0, c.stream>>>(
       c.gaunt.as<float>(), G, rho, u, xe, n, z, dL, emin, emax, num_samples, out, out_stride);
+  ++c.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t quantity_xray_photon_flux_launch(Context& c, const float* rho, const float* u,
+                                             const float* xe, uint64_t n, float z, float dL,
+                                             float emin, float emax, int num_samples,
+                                             float* out) {
+  GauntView G{c.gw, c.gh, c.gx0, c.gy0, c.gdx, c.gdy};
+  xray_flux_kernel<true><<<persistent_blocks(n), 256, 0, c.stream>>>(
+      c.gaunt.as<float>(), G, rho, u, xe, n, z, dL, emin, emax, num_samples, out, 1);
+  ++c.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t quantity_chandra_total_launch(Context& c, const float* rho, const float* u,
+                                          const float* xe, uint64_t n, float z, float dL,
+                                          float* out) {
+  GauntView G{c.gw, c.gh, c.gx0, c.gy0, c.gdx, c.gdy};
+  ArfView A{c.arf_n, c.arf_x0, c.arf_dx};
+  chandra_total_kernel<<<persistent_blocks(n), 256, 0, c.stream>>>(
+      c.gaunt.as<float>(), G, c.arf.as<float>(), A, rho, u, xe, n, z, dL, out);
+  ++c.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t quantity_chandra_bin_launch(Context& c, const float* rho, const float* u,
+                                        const float* xe, uint64_t n, float z, float dL, float e,
+                                        float de, float* out) {
+  GauntView G{c.gw, c.gh, c.gx0, c.gy0, c.gdx, c.gdy};
+  ArfView A{c.arf_n, c.arf_x0, c.arf_dx};
+  chandra_bin_kernel<<<persistent_blocks(n), 256, 0, c.stream>>>(
+      c.gaunt.as<float>(), G, c.arf.as<float>(), A, rho, u, xe, n, z, dL, e, de, out);
+  ++c.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t quantity_chandra_bins_launch(Context& c, const float* rho, const float* u,
+                                         const float* xe, uint64_t n, float z, float dL,
+                                         const float* e, const float* de, int n_bins,
+                                         float* out) {
+  GauntView G{c.gw, c.gh, c.gx0, c.gy0, c.gdx, c.gdy};
+  ArfView A{c.arf_n, c.arf_x0, c.arf_dx};
+  chandra_bins_kernel<<<persistent_blocks(n * (uint64_t)n_bins), 256, 0, c.stream>>>(
+      c.gaunt.as<float>(), G, c.arf.as<float>(), A, rho, u, xe, n, z, dL, e, de, n_bins, out);
   ++c.launches;
   return cudaGetLastError();
 }

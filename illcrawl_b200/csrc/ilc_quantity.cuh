@@ -70,8 +70,10 @@ __device__ __forceinline__ float brems(const float* t, const GauntView& G, float
          r2;
 }
 
-// integrate_spectral_flux(XRAY_FLUX): (rel_tol, 1) passed as (absolute,
-// relative) tolerance, epsilon 0, step bounds [1e-3, 100].
+// integrate_spectral_flux (quantities.cl:156-239): (rel_tol, 1) passed as
+// (absolute, relative) tolerance, epsilon 0, step bounds [1e-3, 100].
+// kPhoton = PHOTON_FLUX: every emission sample is divided by its energy.
+template <bool kPhoton = false>
 __device__ __forceinline__ float band_flux(const float* t, const GauntView& G, float Emin,
                                            float Emax, float reltol, float T, float xe,
                                            float rho, float dL) {
@@ -79,17 +81,56 @@ __device__ __forceinline__ float band_flux(const float* t, const GauntView& G, f
   const float end = Emax;
   float dE = (end - E) * reltol;
   float k1 = brems(t, G, E, 1.0f, T, xe, rho, dL);
+  if (kPhoton) k1 = k1 / E;
   float p[4];
   rkf_points(E, dE, p);
   int guard = 0;
   while (E < end && guard < 100000) {
     float v[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) v[j] = brems(t, G, p[j], 1.0f, T, xe, rho, dL);
+    for (int j = 0; j < 4; ++j) {
+      v[j] = brems(t, G, p[j], 1.0f, T, xe, rho, dL);
+      if (kPhoton) v[j] = v[j] / p[j];
+    }
     rkf_advance_ref32(em, E, dE, k1, reltol, 1.0f, end, v, 0.0f, 1.e-3f, 100.f, p);
     ++guard;
   }
   return em;
+}
+
+// A 1D tabulated function (util::tabulated_function, tabulated_function.hpp:
+// 35-103): n samples from x0 in steps of dx. Used for the Chandra ARF.
+struct ArfView {
+  int n;
+  float x0, dx;
+};
+
+// evaluate_tabulated_function (tabulated_function.cl:31-44): the 1D form of
+// the software image lookup above; samples outside the table read 0.
+__device__ __forceinline__ float tab1d(const float* __restrict__ t, const ArfView& A, float x) {
+  float u = (x - A.x0) / A.dx;
+  if (!(u == u)) return 0.0f;
+  u = fminf(fmaxf(u, -4.0f), (float)(A.n + 4));
+  const float us = u - 0.5f;
+  const float fu = floorf(us);
+  const int i0 = (int)fu;
+  const float a = us - fu;
+  const float t0 = (i0 >= 0 && i0 < A.n) ? __ldg(t + i0) : 0.0f;
+  const float t1 = (i0 + 1 >= 0 && i0 + 1 < A.n) ? __ldg(t + i0 + 1) : 0.0f;
+  return (1.0f - a) * t0 + a * t1;
+}
+
+// get_chandra_xray_count_rate_with_temp (quantities.cl:432-460): the photon
+// count rate of the channel (E, dE) at redshift z times the ARF at E
+// (cm^2 -> m^2), get_spectral_brems_count_rate (quantities.cl:251-260) being
+// the emission divided by the redshifted energy.
+__device__ __forceinline__ float chandra_rate(const float* t, const GauntView& G,
+                                              const float* __restrict__ arf, const ArfView& A,
+                                              float E, float dE, float z, float T, float xe,
+                                              float rho, float dL) {
+  const float av = tab1d(arf, A, E) * 1.e-4f;
+  const float Ez = (1.f + z) * E;
+  return brems(t, G, Ez, (1.f + z) * dE, T, xe, rho, dL) / Ez * av;
 }
 
 }  // namespace ilc

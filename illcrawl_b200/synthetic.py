@@ -176,3 +176,33 @@ def gaussian_random_field_at(pos, box, sigma=0.1, ell=200.0, n=256, seed=20174):
 def perturbed_internal_energy(cells, field):
     """u for log T + field (T is proportional to u at fixed x_e)."""
     return (cells.u.astype(np.float64) * np.exp(field)).astype(np.float32)
+
+
+def synthetic_arf(n=1024, x_min=0.105322271585, dx=0.010644, seed=20175):
+    """A seeded stand-in for an X-ray telescope's effective area [cm^2] on the
+    reference ARF's energy grid (n samples from x_min in steps of dx): a
+    log-normal bump peaking near 1.3 keV, an absorption edge at 2.1 keV, next
+    to nothing below 0.25 keV, and 1 % sample noise. The reference's own
+    table (the Chandra Cycle 19 ACIS-I ARF) lives in its sources; this
+    library loads whatever table the caller passes to ``ilc_arf_load``."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    e = x_min + dx * np.arange(n, dtype=np.float64)
+    area = 600.0 * np.exp(-((np.log(e) - np.log(1.3)) / 0.9) ** 2)
+    area *= np.where(e > 2.1, 0.8, 1.0)
+    area *= 1.0 / (1.0 + np.exp(-(e - 0.3) / 0.03))
+    area *= 1.0 + 0.01 * rng.standard_normal(n)
+    return area.astype(np.float32)
+
+
+def chandra_spectrum_channels(num_frames, arf_min_energy=0.1053223, arf_num_bins=1024,
+                              arf_bin_width=0.010644):
+    """Channel energies and widths of the frames of a Chandra spectrum
+    (chandra_spectrum_quantity_generator::operator(), spectrum.cpp:45-65):
+    frame i sits at arf_min + i * (arf_max - arf_min) / num_frames, computed
+    in double, with the width of one ARF bin; arf_max = arf_min +
+    arf_num_bins * arf_bin_width (chandra::arf::arf_max_energy). Defaults: the
+    reference's arf_min_energy(), get_num_arf_bins() and arf_bin_width()."""
+    arf_max = arf_min_energy + arf_num_bins * arf_bin_width
+    width = (arf_max - arf_min_energy) / float(num_frames)
+    e = np.array([arf_min_energy + i * width for i in range(num_frames)], np.float64)
+    return e.astype(np.float32), np.full(num_frames, arf_bin_width, np.float32)

@@ -37,7 +37,8 @@ typedef enum ilc_status {
   ILC_ERR_STEP_LIMIT = 6,      /* a ray reached the per-ray RKF step cap */
   ILC_ERR_NONFINITE_INPUT = 7, /* NaN or Inf particle coordinates */
   ILC_ERR_GRID_TOO_LARGE = 8,  /* more than 2^32 grid cells or 2^31 particles */
-  ILC_ERR_INTERNAL = 9
+  ILC_ERR_INTERNAL = 9,
+  ILC_ERR_NO_ARF_TABLE = 10    /* Chandra quantity before ilc_arf_load */
 } ilc_status;
 
 typedef struct ilc_ctx ilc_ctx;
@@ -191,6 +192,49 @@ ilc_status ilc_quantity_xray_spectrum(ilc_ctx* ctx, const float* rho, const floa
                                       float luminosity_distance, const float* energies,
                                       const float* widths, int32_t n_bins, float* out,
                                       int is_device);
+
+/* Per-cell photon flux [photons/s/kpc^3/cm^2]: the xray_photon_flux kernel
+ * (quantities.cl:640-675), i.e. xray_flux's energy integral of the emission
+ * divided by the photon energy, times 1e-4 (per m^2 -> per cm^2). */
+ilc_status ilc_quantity_xray_photon_flux(ilc_ctx* ctx, const float* rho, const float* u,
+                                         const float* xe, uint64_t n, float redshift,
+                                         float luminosity_distance, float e_min, float e_max,
+                                         int32_t num_samples, float* out, int is_device);
+
+/* Chandra effective area: n samples [cm^2] from energy x_min [keV] in steps
+ * of dx, as util::tabulated_function holds chandra::arf (tabulated_function.hpp:
+ * 35-103; chandra.cpp, the Cycle 19 ACIS-I ARF: 1024 samples, x_min 0.105322271585,
+ * dx 0.010644). The table is the caller's: the reference keeps it in its
+ * sources and this library ships none. At most 65536 samples. */
+ilc_status ilc_arf_load(ilc_ctx* ctx, const float* table, int32_t n, float x_min, float dx);
+
+/* Per-cell Chandra count rate [counts/s/kpc^3]: chandra_xray_total_count_rate
+ * (quantities.cl:510-557), the count rate of every ARF channel k (energy
+ * x_min + k dx, width dx) summed in channel order. Needs ilc_gaunt_load and
+ * ilc_arf_load. */
+ilc_status ilc_quantity_chandra_count_rate(ilc_ctx* ctx, const float* rho, const float* u,
+                                           const float* xe, uint64_t n, float redshift,
+                                           float luminosity_distance, float* out,
+                                           int is_device);
+
+/* Per-cell Chandra count rate in one channel (energy, energy_bin_width [keV]):
+ * chandra_xray_spectral_count_rate (quantities.cl:584-622). */
+ilc_status ilc_quantity_chandra_spectral_count_rate(ilc_ctx* ctx, const float* rho,
+                                                    const float* u, const float* xe,
+                                                    uint64_t n, float redshift,
+                                                    float luminosity_distance, float energy,
+                                                    float energy_bin_width, float* out,
+                                                    int is_device);
+
+/* Per-cell Chandra count rate in n_bins channels at once, cell-major
+ * out[i * n_bins + b] (the per-frame quantity of
+ * chandra_spectrum_quantity_generator, spectrum.cpp:45-65, in the layout
+ * ilc_render_batched reads). energies, widths: host arrays. */
+ilc_status ilc_quantity_chandra_spectrum(ilc_ctx* ctx, const float* rho, const float* u,
+                                         const float* xe, uint64_t n, float redshift,
+                                         float luminosity_distance, const float* energies,
+                                         const float* widths, int32_t n_bins, float* out,
+                                         int is_device);
 
 /* Per-cell temperature [K]: mean_temperature (quantities.cl:268-284). */
 ilc_status ilc_quantity_temperature(ilc_ctx* ctx, const float* u, const float* xe, uint64_t n,

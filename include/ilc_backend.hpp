@@ -142,11 +142,27 @@ inline std::vector<particle> ingest_cells(context& ctx, const std::vector<float>
   return out;
 }
 
-// spectrum_generator / multi_quantity_integrated_projection
-// (spectrum.hpp:81-126, animation.cpp:264-283) for X-ray spectra: the per-cell
-// bin table and one batched render of every camera. The particles (cell
-// positions) must be set up; rho, u, xe are the cells' fields in that order.
-// cube: per camera, n_bins slices of num_pix_y x num_pix_x.
+// multi_quantity_integrated_projection (animation.cpp:264-283) over a per-cell
+// table of n_bins quantities (cell-major, n x n_bins): one batched render of
+// every camera. cube: per camera, n_bins slices of num_pix_y x num_pix_x.
+inline ilc_render_stats render_table(context& ctx, const std::vector<float>& table, int32_t nb,
+                                     std::vector<ilc_job>& jobs, double rel_tol,
+                                     std::vector<float>& cube) {
+  uint64_t off = 0;
+  for (auto& j : jobs) {
+    j.out_offset = off;
+    off += (uint64_t)nb * (uint64_t)j.camera.num_pix_x * (uint64_t)j.camera.num_pix_y;
+  }
+  cube.assign(off, 0.0f);
+  ilc_render_stats st{};
+  ctx.check(ilc_render_batched(ctx.get(), table.data(), nb, 0, jobs.data(), (int32_t)jobs.size(),
+                               ilc_tolerance{0.0, rel_tol}, cube.data(), off, 0, &st));
+  return st;
+}
+
+// spectrum_generator (spectrum.hpp:81-126) for X-ray spectra: the per-cell
+// bin table, then render_table. The particles (cell positions) must be set
+// up; rho, u, xe are the cells' fields in that order.
 inline ilc_render_stats render_xray_spectra(context& ctx, const std::vector<float>& rho,
                                             const std::vector<float>& u,
                                             const std::vector<float>& xe, float redshift,
@@ -161,16 +177,32 @@ inline ilc_render_stats render_xray_spectra(context& ctx, const std::vector<floa
   ctx.check(ilc_quantity_xray_spectrum(ctx.get(), rho.data(), u.data(), xe.data(), n, redshift,
                                        luminosity_distance, energies.data(), widths.data(), nb,
                                        table.data(), 0));
-  uint64_t off = 0;
-  for (auto& j : jobs) {
-    j.out_offset = off;
-    off += (uint64_t)nb * (uint64_t)j.camera.num_pix_x * (uint64_t)j.camera.num_pix_y;
-  }
-  cube.assign(off, 0.0f);
-  ilc_render_stats st{};
-  ctx.check(ilc_render_batched(ctx.get(), table.data(), nb, 0, jobs.data(), (int32_t)jobs.size(),
-                               ilc_tolerance{0.0, rel_tol}, cube.data(), off, 0, &st));
-  return st;
+  return render_table(ctx, table, nb, jobs, rel_tol, cube);
+}
+
+// chandra::arf as util::tabulated_function (tabulated_function.hpp:35-103):
+// the caller's effective-area samples [cm^2] from x_min [keV] in steps of dx.
+inline void load_arf(context& ctx, const std::vector<float>& area, float x_min, float dx) {
+  ctx.check(ilc_arf_load(ctx.get(), area.data(), (int32_t)area.size(), x_min, dx));
+}
+
+// spectrum_generator with chandra_spectrum_quantity_generator (spectrum.cpp:
+// 45-65): channel count rates per cell, then render_table. Needs load_arf.
+inline ilc_render_stats render_chandra_spectra(context& ctx, const std::vector<float>& rho,
+                                               const std::vector<float>& u,
+                                               const std::vector<float>& xe, float redshift,
+                                               float luminosity_distance,
+                                               const std::vector<float>& energies,
+                                               const std::vector<float>& widths,
+                                               std::vector<ilc_job>& jobs, double rel_tol,
+                                               std::vector<float>& cube) {
+  const uint64_t n = rho.size();
+  const int32_t nb = (int32_t)energies.size();
+  std::vector<float> table(n * (uint64_t)nb);
+  ctx.check(ilc_quantity_chandra_spectrum(ctx.get(), rho.data(), u.data(), xe.data(), n,
+                                          redshift, luminosity_distance, energies.data(),
+                                          widths.data(), nb, table.data(), 0));
+  return render_table(ctx, table, nb, jobs, rel_tol, cube);
 }
 
 // volumetric_slice::create_slice (volumetric_slice.cpp:31-101), one sample per

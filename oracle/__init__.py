@@ -63,6 +63,14 @@ def _declare(L):
                                 ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
     L.orc_xray_bin.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, i64, f32, f32, f32, f32,
                                ctypes.c_int, P, ctypes.c_int]
+    L.orc_xray_photon_flux.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, i64, f32, f32,
+                                       f32, f32, ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
+    L.orc_chandra_count_rate.argtypes = [P, ctypes.c_int, ctypes.c_int, P, ctypes.c_int, f32,
+                                         f32, P, P, P, i64, f32, f32, ctypes.c_int, P,
+                                         ctypes.c_int]
+    L.orc_chandra_spectral_count_rate.argtypes = [P, ctypes.c_int, ctypes.c_int, P,
+                                                  ctypes.c_int, f32, f32, P, P, P, i64, f32,
+                                                  f32, f32, f32, ctypes.c_int, P, ctypes.c_int]
 
 
 def _p(a):
@@ -212,6 +220,44 @@ def xray_bin(table, rho, u, xe, z, dL, E, dE, precision=0, nthreads=0):
     out = np.zeros_like(rho)
     lib().orc_xray_bin(_p(t), t.shape[1], t.shape[0], _p(rho), _p(u), _p(xe), rho.size, z, dL,
                        E, dE, precision, _p(out), nthreads)
+    return out
+
+
+def xray_photon_flux(table, rho, u, xe, z, dL, Emin, Emax, num_samples, precision=0,
+                     nthreads=0):
+    """xray_photon_flux (quantities.cl:640-675) per cell [photons/s/kpc^3/cm^2]."""
+    t = np.ascontiguousarray(table, np.float32)
+    rho, u, xe = (np.ascontiguousarray(a, np.float32) for a in (rho, u, xe))
+    out = np.zeros_like(rho)
+    lib().orc_xray_photon_flux(_p(t), t.shape[1], t.shape[0], _p(rho), _p(u), _p(xe), rho.size,
+                               z, dL, Emin, Emax, num_samples, precision, _p(out), nthreads)
+    return out
+
+
+def chandra_count_rate(table, arf, arf_x0, arf_dx, rho, u, xe, z, dL, precision=0, nthreads=0):
+    """chandra_xray_total_count_rate (quantities.cl:510-557) per cell: the
+    count rates of all ARF channels x0 + k dx (width dx) summed in order."""
+    t = np.ascontiguousarray(table, np.float32)
+    a = np.ascontiguousarray(arf, np.float32)
+    rho, u, xe = (np.ascontiguousarray(v, np.float32) for v in (rho, u, xe))
+    out = np.zeros_like(rho)
+    lib().orc_chandra_count_rate(_p(t), t.shape[1], t.shape[0], _p(a), a.size, arf_x0, arf_dx,
+                                 _p(rho), _p(u), _p(xe), rho.size, z, dL, precision, _p(out),
+                                 nthreads)
+    return out
+
+
+def chandra_spectral_count_rate(table, arf, arf_x0, arf_dx, rho, u, xe, z, dL, E, dE,
+                                precision=0, nthreads=0):
+    """chandra_xray_spectral_count_rate (quantities.cl:584-622) per cell for
+    the channel (E, dE)."""
+    t = np.ascontiguousarray(table, np.float32)
+    a = np.ascontiguousarray(arf, np.float32)
+    rho, u, xe = (np.ascontiguousarray(v, np.float32) for v in (rho, u, xe))
+    out = np.zeros_like(rho)
+    lib().orc_chandra_spectral_count_rate(_p(t), t.shape[1], t.shape[0], _p(a), a.size, arf_x0,
+                                          arf_dx, _p(rho), _p(u), _p(xe), rho.size, z, dL, E, dE,
+                                          precision, _p(out), nthreads)
     return out
 
 

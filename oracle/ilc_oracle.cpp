@@ -722,25 +722,71 @@ static inline R brems(const Gaunt& G, R E, R dE, R T, R xe, R rho, R r) {
   return (R)C::pref() * dE * Z * Z * ion * ion * g_ff<R>(G, E, T, Z) * rs *
          mathf<R>::exp(-E * Tinv) / r2;
 }
-// integrate_spectral_flux with type XRAY_FLUX (quantities.cl:156-239): the
-// call of rkf_advance passes (rel_tol, 1) as (absolute, relative) tolerance,
-// epsilon 0, step bounds [1e-3, 100].
+// integrate_spectral_flux (quantities.cl:156-239): the call of rkf_advance
+// passes (rel_tol, 1) as (absolute, relative) tolerance, epsilon 0, step
+// bounds [1e-3, 100]. photon (type PHOTON_FLUX): the emission at the range
+// start and at every evaluation point is divided by that energy.
 template <class R>
-static inline R band_flux(const Gaunt& G, R Emin, R Emax, R reltol, R T, R xe, R rho, R dL) {
+static inline R band_flux(const Gaunt& G, R Emin, R Emax, R reltol, R T, R xe, R rho, R dL,
+                          bool photon = false) {
   R em = (R)0, E = Emin;
   const R end = Emax;
   R dE = (end - E) * reltol;
   R k1 = brems<R>(G, E, (R)1, T, xe, rho, dL);
+  if (photon) k1 /= E;
   R p[4];
   rkf_points<R>(E, dE, p);
   int guard = 0;
   while (E < end && guard < 100000) {
     R v[4];
-    for (int j = 0; j < 4; ++j) v[j] = brems<R>(G, p[j], (R)1, T, xe, rho, dL);
+    for (int j = 0; j < 4; ++j) {
+      v[j] = brems<R>(G, p[j], (R)1, T, xe, rho, dL);
+      if (photon) v[j] /= p[j];
+    }
     rkf_advance_ref<R>(em, E, dE, k1, reltol, (R)1, end, v, (R)0, (R)1.e-3f, (R)100, p);
     ++guard;
   }
   return em;
+}
+
+// util::tabulated_function (tabulated_function.hpp:35-103): n samples from x0
+// in steps of dx; the Chandra ARF (chandra.cpp, chandra::arf) is one.
+struct Arf {
+  const float* t;
+  int n;
+  float x0, dx;
+};
+
+// evaluate_tabulated_function (tabulated_function.cl:31-44): read_imagef on a
+// 1D CL_R image with the same sampler as the Gaunt table (texel centres at
+// i + 0.5, linear blend, border 0).
+template <class R> static inline R arf_sample(const Arf& A, R x) {
+  typedef mathf<R> M;
+  R u = (x - (R)A.x0) / (R)A.dx;
+  if (!(u == u)) return (R)0;
+  u = std::min(std::max(u, (R)-4), (R)(A.n + 4));
+  const R us = u - (R)0.5;
+  const R fu = M::floor(us);
+  const int i0 = (int)fu;
+  const R a = us - fu;
+  const R t0 = (i0 >= 0 && i0 < A.n) ? (R)A.t[i0] : (R)0;
+  const R t1 = (i0 + 1 >= 0 && i0 + 1 < A.n) ? (R)A.t[i0 + 1] : (R)0;
+  return ((R)1 - a) * t0 + a * t1;
+}
+
+template <class R> static inline R cm2_to_m2();
+template <> inline float cm2_to_m2<float>() { return 1.e-4f; }
+template <> inline double cm2_to_m2<double>() { return 1.e-4; }
+
+// get_chandra_xray_count_rate_with_temp (quantities.cl:432-460) with
+// get_spectral_brems_count_rate (quantities.cl:251-260): emission at the
+// redshifted channel / redshifted energy * ARF(E) [cm^2 -> m^2].
+template <class R>
+static inline R chandra_rate(const Gaunt& G, const Arf& A, R E, R dE, R z, R T, R xe, R rho,
+                             R dL) {
+  const R av = arf_sample<R>(A, E) * cm2_to_m2<R>();
+  const R Ez = ((R)1 + z) * E;
+  return brems<R>(G, Ez, ((R)1 + z) * dE, T, xe, rho, dL) / Ez * av;
 }
 
 // ---- derivatives for the adjoint -------------------------------------------
@@ -1524,6 +1570,81 @@ int orc_xray_bin(const float* table, int w, int hgt, const float* rho, const flo
   return 0;
 }
 
+
+// xray_photon_flux kernel (quantities.cl:640-675): photons/s/kpc^3/cm^2.
+int orc_xray_photon_flux(const float* table, int w, int hgt, const float* rho, const float* u,
+                         const float* xe, int64_t n, float z, float dL, float Emin, float Emax,
+                         int num_samples, int precision, float* out, int nthreads) {
+  Gaunt G = make_gaunt(table, w, hgt);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    if (precision == 0) {
+      const float T = temperature<float>(u[i], xe[i]);
+      out[i] = band_flux<float>(G, (1.f + z) * Emin, (1.f + z) * Emax, 1.f / (float)num_samples,
+                                T, xe[i], rho[i], dL, true) * 1.e-4f;
+    } else {
+      const double T = temperature<double>(u[i], xe[i]);
+      const double zz = z;
+      out[i] = (float)(band_flux<double>(G, (1. + zz) * Emin, (1. + zz) * Emax,
+                                         1. / (double)num_samples, T, xe[i], rho[i], dL, true) *
+                       1.e-4);
+    }
+  }
+  return 0;
+}
+
+// chandra_xray_total_count_rate kernel (quantities.cl:510-557): the channel
+// count rates of every ARF channel k (energy x0 + k * dx, width dx) summed in
+// channel order.
+int orc_chandra_count_rate(const float* table, int w, int hgt, const float* arf, int n_arf,
+                           float ax0, float adx, const float* rho, const float* u,
+                           const float* xe, int64_t n, float z, float dL, int precision,
+                           float* out, int nthreads) {
+  Gaunt G = make_gaunt(table, w, hgt);
+  const Arf A{arf, n_arf, ax0, adx};
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    if (precision == 0) {
+      const float T = temperature<float>(u[i], xe[i]);
+      float em = 0.0f;
+      for (int k = 0; k < n_arf; ++k)
+        em += chandra_rate<float>(G, A, ax0 + (float)k * adx, adx, z, T, xe[i], rho[i], dL);
+      out[i] = em;
+    } else {
+      const double T = temperature<double>(u[i], xe[i]);
+      double em = 0.0;
+      for (int k = 0; k < n_arf; ++k)
+        em += chandra_rate<double>(G, A, (double)ax0 + (double)k * (double)adx, (double)adx,
+                                   (double)z, T, xe[i], rho[i], dL);
+      out[i] = (float)em;
+    }
+  }
+  return 0;
+}
+
+// chandra_xray_spectral_count_rate kernel (quantities.cl:584-622): one channel.
+int orc_chandra_spectral_count_rate(const float* table, int w, int hgt, const float* arf,
+                                    int n_arf, float ax0, float adx, const float* rho,
+                                    const float* u, const float* xe, int64_t n, float z,
+                                    float dL, float E, float dE, int precision, float* out,
+                                    int nthreads) {
+  Gaunt G = make_gaunt(table, w, hgt);
+  const Arf A{arf, n_arf, ax0, adx};
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    if (precision == 0) {
+      const float T = temperature<float>(u[i], xe[i]);
+      out[i] = chandra_rate<float>(G, A, E, dE, z, T, xe[i], rho[i], dL);
+    } else {
+      const double T = temperature<double>(u[i], xe[i]);
+      out[i] = (float)chandra_rate<double>(G, A, E, dE, z, T, xe[i], rho[i], dL);
+    }
+  }
+  return 0;
+}
 
 // Batched render (see Job). values: n x V, cell-major, original cell order.
 // rays == nullptr: every pixel of every job into images at the job offsets

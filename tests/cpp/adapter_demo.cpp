@@ -82,6 +82,11 @@ int main() {
       ilc::render_xray_spectra(ctx, krho, ku, kxe, 0.2f, 978500.0f, {1.0f, 2.0f}, {1.0f, 1.0f},
                                jobs, 1e-3, cube);
       for (float v : cube) sum += v * 1e-20;
+      // a flat 100 cm^2 effective area over 0.1-6.5 keV in place of the Chandra ARF
+      ilc::load_arf(ctx, std::vector<float>(64, 100.0f), 0.1f, 0.1f);
+      ilc::render_chandra_spectra(ctx, krho, ku, kxe, 0.2f, 978500.0f, {0.5f, 2.0f},
+                                  {0.1f, 0.1f}, jobs, 1e-3, cube);
+      for (float v : cube) sum += v * 1e-20;
     } catch (const ilc::error& e) {
       if (e.status != ILC_ERR_NO_GAUNT_TABLE) throw;  // run from elsewhere: no table file
     }
