@@ -61,7 +61,8 @@ def test_chandra_count_rates_bit_exact(ctx, oracle_mod, gaunt_table, arf):
     tot = ctx.chandra_count_rate(c.rho, c.u, c.xe, Z, DL)
     otot = oracle_mod.chandra_count_rate(gaunt_table, arf, X0, DX, c.rho, c.u, c.xe, Z, DL)
     assert same_bits(tot, otot)
-    assert np.all(tot > 0)
+    # cold, thin background cells underflow to 0 in fp32, as in the oracle
+    assert np.all(tot >= 0) and np.count_nonzero(tot) > tot.size // 2
     # channels inside, on the edges of and outside the table
     for e in (X0, 0.4, 1.3, 2.1, X0 + 1023.7 * DX, X0 + 1030 * DX, 0.01):
         r = ctx.chandra_spectral_count_rate(c.rho, c.u, c.xe, e, DX, Z, DL)
