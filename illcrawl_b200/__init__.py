@@ -22,7 +22,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import (CONTROLLER_FP64, CONTROLLER_REF32, DA_INVERSE_RANGE, DA_PIXEL_AREA, DA_UNIT,
-                   ENGINE_GRID, ENGINE_PERSISTENT, Camera, IlcError, Job, LosScaling, RenderStats, Tolerance)
+                   DV_MEAN, DV_VOLUME, ENGINE_GRID, ENGINE_PERSISTENT, Camera, IlcError, Job,
+                   LosScaling, RenderStats, Tolerance)
 
 DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 GAUNT_FILE = os.path.join(DATA_DIR, "gaunt_factor.dat")
@@ -122,6 +123,19 @@ def write_fits(path, data, cards=()):
                                 len(cards))
     if st:
         raise IlcError(st, f"could not write {path}")
+
+
+def mc_profile_shells(max_radius, num_radii, sample_density):
+    """Shell radii and per-shell sample counts of a Monte-Carlo radial profile
+    (ilc_mc_profile_shells; host only)."""
+    radii = np.zeros(num_radii, np.float64)
+    counts = np.zeros(num_radii, np.uint64)
+    st = _lib.load().ilc_mc_profile_shells(float(max_radius), int(num_radii),
+                                            float(sample_density), _ptr(radii), _ptr(counts))
+    if st != _lib.ILC_OK:
+        raise IlcError(st, "invalid profile shells (radius, 1..2^20 radii, density, at most "
+                           "2^40 samples)")
+    return radii, counts
 
 
 def camera_plane(cam):
@@ -433,6 +447,25 @@ class Context:
                                                     int(initial_z_step), int(num_steps),
                                                     _ptr(cube), 0))
         return cube
+
+    # ---- Monte-Carlo radial profiles
+    def mc_radial_profile(self, center, max_radius, num_radii, sample_density, seed=0,
+                          dV_mode=DV_VOLUME, volume_conversion=1.0, samples=False):
+        """distributed_mc_radial_profile of the particles' q around center
+        (ilc_mc_radial_profile): the profile (num_radii doubles), and with
+        samples=True also every sample point (total, 4) and value (total,)."""
+        c = np.ascontiguousarray(center, np.float64)
+        prof = np.zeros(num_radii, np.float64)
+        pts = vals = None
+        if samples:
+            total = int(mc_profile_shells(max_radius, num_radii, sample_density)[1].sum())
+            pts = np.zeros((total, 4), np.float32)
+            vals = np.zeros(total, np.float32)
+        self.check(self.L.ilc_mc_radial_profile(self.h, _ptr(c), float(max_radius), int(num_radii),
+                                                float(sample_density), int(seed), int(dV_mode),
+                                                float(volume_conversion), _ptr(prof), _ptr(pts),
+                                                _ptr(vals)))
+        return (prof, pts, vals) if samples else prof
 
     # ---- cell ingestion
     def ingest_cells(self, xyz, q, center, extent, periodic, border=100.0):

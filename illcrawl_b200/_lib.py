@@ -20,6 +20,7 @@ STATUS_NAMES = {
 CONTROLLER_REF32 = 0
 CONTROLLER_FP64 = 1
 DA_PIXEL_AREA, DA_UNIT, DA_INVERSE_RANGE = 0, 1, 2
+DV_VOLUME, DV_MEAN = 0, 1
 ENGINE_GRID, ENGINE_PERSISTENT = 0, 1
 
 
@@ -127,6 +128,8 @@ SIGNATURES = {
     "ilc_quantity_xray_photon_flux": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32,
                                              _P, _int]),
     "ilc_arf_load": (_int, [_P, _P, _i32, _f32, _f32]),
+    "ilc_mc_profile_shells": (_int, [_f64, _i32, _f64, _P, _P]),
+    "ilc_mc_radial_profile": (_int, [_P, _P, _f64, _i32, _f64, _u64, _i32, _f64, _P, _P, _P]),
     "ilc_quantity_chandra_count_rate": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _P, _int]),
     "ilc_quantity_chandra_spectral_count_rate": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _f32,
                                                         _f32, _P, _int]),

@@ -383,6 +383,53 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
   return ILC_OK;
 }
 
+// distributed_mc_radial_profile's shells (profile.cpp:320-355) and
+// generate_num_samples (profile.cpp:93-128), in the reference's double
+// arithmetic and summation order.
+struct ProfileShells {
+  std::vector<double> radius, r_min, r_max, volume;
+  std::vector<uint64_t> count, prefix;  // prefix: num_radii + 1 entries
+};
+
+constexpr uint64_t kMaxProfileSamples = 1ull << 40;
+constexpr uint64_t kProfileSegment = 8192;       // samples per reduction segment
+constexpr uint64_t kProfileBatch = 1ull << 22;   // samples per device batch
+
+bool profile_shells(double max_radius, int32_t num_radii, double density, ProfileShells* S) {
+  if (!(max_radius > 0.0) || !std::isfinite(max_radius) || num_radii < 1 ||
+      num_radii > (1 << 20) || !(density > 0.0) || !std::isfinite(density))
+    return false;
+  const unsigned N = (unsigned)num_radii;
+  auto radius = [&](unsigned i) { return i * (max_radius / N); };
+  S->radius.resize(N);
+  S->r_min.resize(N);
+  S->r_max.resize(N);
+  S->volume.resize(N);
+  for (unsigned i = 0; i < N; ++i) {
+    S->radius[i] = radius(i);
+    S->r_min[i] = i == 0 ? 0.0 : 0.5 * (radius(i - 1) + radius(i));
+    S->r_max[i] = 0.5 * (radius(i + 1) + radius(i));
+    const double a = S->r_min[i], b = S->r_max[i];
+    S->volume[i] = 4. / 3 * M_PI * (b * b * b - a * a * a);
+  }
+  double expected = 0.0, sum_sq = 0.0;
+  for (unsigned i = 0; i < N; ++i) expected += S->volume[i] * density;
+  for (unsigned i = 0; i < N; ++i) sum_sq += S->volume[i] * S->volume[i];
+  const double norm = expected / sum_sq;
+  S->count.resize(N);
+  S->prefix.assign(N + 1, 0);
+  for (unsigned i = 0; i < N; ++i) {
+    const double want = norm * (S->volume[i] * S->volume[i]);
+    if (!(want < (double)kMaxProfileSamples)) return false;
+    uint64_t n = (uint64_t)want;
+    if (n == 0) n = 1;
+    S->count[i] = n;
+    S->prefix[i + 1] = S->prefix[i] + n;
+    if (S->prefix[i + 1] > kMaxProfileSamples) return false;
+  }
+  return true;
+}
+
 }  // namespace
 }  // namespace ilc
 
@@ -428,7 +475,8 @@ void ilc_destroy(ilc_ctx* h) {
                     &c.in_b, &c.in_c, &c.out_a, &c.out_b, &c.out_c, &c.spiral, &c.flags,
                     &c.rec_h, &c.rec_n, &c.adj_dT, &c.adj_dR, &c.adj_grad, &c.adj_seed,
                     &c.adj_loss, &c.codes, &c.jobs, &c.chan_sorted, &c.chan_state, &c.queue,
-                    &c.item_cost, &c.item_order, &c.arf})
+                    &c.item_cost, &c.item_order, &c.arf, &c.prof_tab, &c.prof_seg,
+                    &c.prof_sum})
     b->release();
   if (c.batch_exec) cudaGraphExecDestroy(c.batch_exec);
   if (c.ev0) cudaEventDestroy(c.ev0);
@@ -1374,6 +1422,111 @@ ilc_status ilc_volumetric_tomography(ilc_ctx* h, const ilc_camera* cam, double d
              "tomography slice");
   }
   ILC_CUDA(c, finish_out(c, cube, dcube, npix * (uint64_t)num_steps * 4, is_device), "tomography");
+  return ILC_OK;
+}
+
+ilc_status ilc_mc_profile_shells(double max_radius, int32_t num_radii, double sample_density,
+                                 double* radii, uint64_t* counts) {
+  ProfileShells S;
+  if (!profile_shells(max_radius, num_radii, sample_density, &S))
+    return ILC_ERR_INVALID_ARGUMENT;
+  for (int32_t i = 0; i < num_radii; ++i) {
+    if (radii) radii[i] = S.radius[i];
+    if (counts) counts[i] = S.count[i];
+  }
+  return ILC_OK;
+}
+
+ilc_status ilc_mc_radial_profile(ilc_ctx* h, const double center[3], double max_radius,
+                                 int32_t num_radii, double sample_density, uint64_t seed,
+                                 int32_t dV_mode, double volume_conversion, double* profile,
+                                 float* sample_points, float* sample_values) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "profile before setup_particles");
+  if (!center || !profile || (dV_mode != ILC_DV_VOLUME && dV_mode != ILC_DV_MEAN) ||
+      !std::isfinite(center[0]) || !std::isfinite(center[1]) || !std::isfinite(center[2]) ||
+      !std::isfinite(volume_conversion))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid profile arguments");
+  ProfileShells S;
+  if (!profile_shells(max_radius, num_radii, sample_density, &S))
+    return fail(c, ILC_ERR_INVALID_ARGUMENT,
+                "invalid profile shells (radius, 1..2^20 radii, density, at most 2^40 samples)");
+  const uint32_t N = (uint32_t)num_radii;
+  // device shell table: prefix (N + 1), u_min (N), u_max (N)
+  std::vector<char> tab(8 * (size_t)(N + 1) + 16 * (size_t)N);
+  uint64_t* t_prefix = reinterpret_cast<uint64_t*>(tab.data());
+  double* t_umin = reinterpret_cast<double*>(tab.data() + 8 * (size_t)(N + 1));
+  double* t_umax = t_umin + N;
+  for (uint32_t i = 0; i <= N; ++i) t_prefix[i] = S.prefix[i];
+  for (uint32_t i = 0; i < N; ++i) {
+    // uniform_spherical_shell's u range (random.cpp:67-74)
+    t_umin[i] = S.r_min[i] * S.r_min[i] * S.r_min[i];
+    t_umax[i] = S.r_max[i] * S.r_max[i] * S.r_max[i];
+  }
+  // reduction segments: at most kProfileSegment consecutive samples of one shell
+  std::vector<ulonglong2> segs;
+  std::vector<uint32_t> seg_shell;
+  for (uint32_t i = 0; i < N; ++i)
+    for (uint64_t b = S.prefix[i]; b < S.prefix[i + 1]; b += kProfileSegment) {
+      segs.push_back(make_ulonglong2(b, std::min(b + kProfileSegment, S.prefix[i + 1])));
+      seg_shell.push_back(i);
+    }
+  const uint64_t total = S.prefix[N];
+  const uint64_t batch_cap = std::min(total, kProfileBatch);
+  ILC_CUDA(c, c.prof_tab.ensure(tab.size()), "profile table");
+  ILC_CUDA(c, c.prof_seg.ensure(segs.size() * sizeof(ulonglong2)), "profile segments");
+  ILC_CUDA(c, c.prof_sum.ensure(segs.size() * 8), "profile sums");
+  ILC_CUDA(c, c.in_b.ensure(batch_cap * 16), "profile points");
+  ILC_CUDA(c, c.out_b.ensure(batch_cap * 4), "profile values");
+  ILC_CUDA(c, cudaMemcpyAsync(c.prof_tab.p, tab.data(), tab.size(), cudaMemcpyHostToDevice,
+                              c.stream), "profile table H2D");
+  ILC_CUDA(c, cudaMemcpyAsync(c.prof_seg.p, segs.data(), segs.size() * sizeof(ulonglong2),
+                              cudaMemcpyHostToDevice, c.stream), "profile segments H2D");
+  const uint64_t* d_prefix = c.prof_tab.as<uint64_t>();
+  const double* d_umin = reinterpret_cast<const double*>(c.prof_tab.as<char>() + 8 * (size_t)(N + 1));
+  const double* d_umax = d_umin + N;
+  size_t si = 0;
+  while (si < segs.size()) {
+    // a batch: the consecutive whole segments that fit in kProfileBatch samples
+    const uint64_t g0 = segs[si].x;
+    size_t sj = si;
+    while (sj < segs.size() && segs[sj].y - g0 <= kProfileBatch) ++sj;
+    const uint64_t n = segs[sj - 1].y - g0;
+    ILC_CUDA(c, profile_points_launch(c, d_prefix, (int)N, d_umin, d_umax, center, seed, g0, n,
+                                      c.in_b.as<float4>()),
+             "profile points kernel");
+    ILC_CUDA(c, nn8_query_launch(c, c.in_b.as<float4>(), n, false, c.out_b.as<float>(), nullptr,
+                                 nullptr),
+             "profile nn8 kernel");
+    ILC_CUDA(c, profile_segment_sum_launch(c, c.prof_seg.as<ulonglong2>() + si,
+                                           (uint32_t)(sj - si), g0, c.out_b.as<float>(),
+                                           c.prof_sum.as<double>() + si),
+             "profile reduction kernel");
+    if (sample_points)
+      ILC_CUDA(c, cudaMemcpyAsync(sample_points + 4 * g0, c.in_b.p, n * 16,
+                                  cudaMemcpyDeviceToHost, c.stream), "profile points D2H");
+    if (sample_values)
+      ILC_CUDA(c, cudaMemcpyAsync(sample_values + g0, c.out_b.p, n * 4, cudaMemcpyDeviceToHost,
+                                  c.stream), "profile values D2H");
+    ILC_CUDA(c, cudaStreamSynchronize(c.stream), "profile batch");
+    si = sj;
+  }
+  std::vector<double> seg_sum(segs.size());
+  ILC_CUDA(c, cudaMemcpyAsync(seg_sum.data(), c.prof_sum.p, segs.size() * 8,
+                              cudaMemcpyDeviceToHost, c.stream), "profile sums D2H");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "profile");
+  for (uint32_t i = 0; i < N; ++i) profile[i] = 0.0;
+  for (size_t k = 0; k < segs.size(); ++k) profile[seg_shell[k]] += seg_sum[k];
+  for (uint32_t i = 0; i < N; ++i) {
+    // apply_volume_factor (profile.cpp:236-256)
+    const double dV = S.volume[i] / (double)S.count[i];
+    const double eff = dV_mode == ILC_DV_VOLUME
+                           ? dV * volume_conversion
+                           : (dV * volume_conversion) / (S.volume[i] * volume_conversion);
+    profile[i] *= eff;
+  }
   return ILC_OK;
 }
 

@@ -92,6 +92,9 @@ struct Context {
   // adjoint: step checkpoints, per-cell derivatives, gradient accumulator
   DevBuf rec_h, rec_n, adj_dT, adj_dR, adj_grad, adj_seed, adj_loss;
 
+  // Monte-Carlo radial profile: shell table, segments, segment sums
+  DevBuf prof_tab, prof_seg, prof_sum;
+
   // batched render: job table, sorted channel table, channel state, queue
   DevBuf jobs, chan_sorted, chan_state, queue, item_cost, item_order;
   int32_t batch_tile_w = 8;       // batched work item: tile_w x (32 / tile_w) pixels
@@ -159,6 +162,12 @@ cudaError_t quantity_xray_bins_launch(Context& c, const float* rho, const float*
                                       const float* e, const float* de, int n_bins, float* out);
 cudaError_t quantity_temperature_launch(Context& c, const float* u, const float* xe,
                                         uint64_t n, float* out);
+cudaError_t profile_points_launch(Context& c, const uint64_t* prefix, int n_shells,
+                                  const double* u_min, const double* u_max,
+                                  const double center[3], uint64_t seed, uint64_t g0, uint64_t n,
+                                  float4* pts);
+cudaError_t profile_segment_sum_launch(Context& c, const ulonglong2* segs, uint32_t n_segs,
+                                       uint64_t g0, const float* vals, double* sums);
 cudaError_t quantity_xray_photon_flux_launch(Context& c, const float* rho, const float* u,
                                              const float* xe, uint64_t n, float z, float dL,
                                              float emin, float emax, int num_samples,

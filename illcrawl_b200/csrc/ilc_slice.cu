@@ -10,6 +10,7 @@
 #include <algorithm>
 
 #include "ilc_internal.h"
+#include "ilc_random.cuh"
 
 namespace ilc {
 namespace {
@@ -19,13 +20,6 @@ struct SlicePlane {
   double ps;
   int nx, ny;
 };
-
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {  // splitmix64 finaliser
-  z += 0x9e3779b97f4a7c15ull;
-  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-  return z ^ (z >> 31);
-}
 
 __device__ __forceinline__ double unit_offset(uint64_t h) {  // [-0.5, 0.5)
   return (double)(h >> 11) * (1.0 / 9007199254740992.0) - 0.5;

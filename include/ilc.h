@@ -329,6 +329,37 @@ ilc_status ilc_volumetric_tomography(ilc_ctx* ctx, const ilc_camera* cam, double
                                      int64_t initial_z_step, int64_t num_steps, float* cube,
                                      int is_device);
 
+/* ---- Monte-Carlo radial profiles ------------------------------------------
+ * distributed_mc_radial_profile (profile.cpp:26-355) on one device.
+ * Shell i of num_radii: radius r_i = i * max_radius / num_radii
+ * (get_comoving_profile_radii), spanning [(r_{i-1} + r_i)/2, (r_i + r_{i+1})/2]
+ * (shell 0 from 0; profile.cpp:320-355), with n_i = max(1, floor(norm V_i^2))
+ * samples, norm = sample_density * sum(V) / sum(V^2) (generate_num_samples,
+ * profile.cpp:93-128). */
+enum { ILC_DV_VOLUME = 0, ILC_DV_MEAN = 1 };
+
+/* Shell radii and sample counts (host only; either output may be NULL).
+ * num_radii in [1, 2^20]; fails when the samples would exceed 2^40. */
+ilc_status ilc_mc_profile_shells(double max_radius, int32_t num_radii, double sample_density,
+                                 double* radii, uint64_t* counts);
+
+/* The profile of the particles' q (ilc_nn8_setup_particles) around center:
+ * per shell, the nn8 values at its samples summed in double, times the
+ * quantity's effective dV of apply_volume_factor (profile.cpp:236-256) with
+ * dV = V_i / n_i: ILC_DV_VOLUME gives dV * volume_conversion (the X-ray
+ * quantities, quantity.hpp:193-197), ILC_DV_MEAN (dV * volume_conversion) /
+ * (V_i * volume_conversion) (density, temperature; quantity.hpp:477-480,
+ * 560-565). Each sample is uniform in its shell (uniform_spherical_shell,
+ * random.cpp:28-86) with its draws hashed from (seed, sample index): the
+ * reference seeds std::mt19937 from std::random_device, so its samples are
+ * never reproducible. profile: num_radii doubles. sample_points (4 floats per
+ * sample) and sample_values (1 float per sample) receive every sample in
+ * order, shells in order; either may be NULL. All outputs are host memory. */
+ilc_status ilc_mc_radial_profile(ilc_ctx* ctx, const double center[3], double max_radius,
+                                 int32_t num_radii, double sample_density, uint64_t seed,
+                                 int32_t dV_mode, double volume_conversion, double* profile,
+                                 float* sample_points, float* sample_values);
+
 /* ---- cell ingestion ---------------------------------------------------------
  * The per-row loop of reconstructing_data_crawler::run
  * (reconstructing_data_crawler.cpp:170-230) on the device: each cell's float

@@ -214,6 +214,27 @@ inline void volumetric_slice(context& ctx, const ilc_camera& cam, double dV,
   ctx.check(ilc_volumetric_slice(ctx.get(), &cam, dV, additional_samples, seed, image.data(), 0));
 }
 
+// distributed_mc_radial_profile::operator() (profile.cpp:47-74) on one device:
+// the profile of the particles' quantity in num_radii shells around center,
+// and the shell radii (get_comoving_profile_radii).
+inline std::vector<double> mc_radial_profile(context& ctx, const std::array<double, 3>& center,
+                                             double max_radius, int32_t num_radii,
+                                             double sample_density, uint64_t seed = 0,
+                                             int32_t dV_mode = ILC_DV_VOLUME,
+                                             double volume_conversion = 1.0,
+                                             std::vector<double>* radii = nullptr) {
+  std::vector<double> profile((std::size_t)num_radii, 0.0);
+  ctx.check(ilc_mc_radial_profile(ctx.get(), center.data(), max_radius, num_radii,
+                                  sample_density, seed, dV_mode, volume_conversion,
+                                  profile.data(), nullptr, nullptr));
+  if (radii) {
+    radii->assign((std::size_t)num_radii, 0.0);
+    ctx.check(ilc_mc_profile_shells(max_radius, num_radii, sample_density, radii->data(),
+                                    nullptr));
+  }
+  return profile;
+}
+
 // util::fits<float>::save + fits_header::add_entry (fits.hpp:142-258).
 inline void write_fits(const std::string& path, const std::vector<float>& data,
                        const std::vector<int64_t>& naxes,

@@ -427,3 +427,49 @@ def volumetric_slice(grid, cam, dV=1.0, nthreads=0):
     out = np.zeros(cam.nx * cam.ny, np.float32)
     L.orc_volumetric_slice(grid.h, ctypes.byref(cam), float(dV), _p(out), nthreads)
     return out.reshape(cam.ny, cam.nx)
+
+
+def _declare_profile(L):
+    P, f64 = ctypes.c_void_p, ctypes.c_double
+    L.orc_mc_profile_shells.argtypes = [f64, ctypes.c_int, f64, P, P]
+    L.orc_mc_radial_profile.argtypes = [P, P, f64, ctypes.c_int, f64, ctypes.c_uint64,
+                                        ctypes.c_int, f64, P, P, P, ctypes.c_int]
+
+
+def _profile_lib():
+    L = lib()
+    if not getattr(L, "_profile_declared", False):
+        _declare_profile(L)
+        L._profile_declared = True
+    return L
+
+
+def mc_profile_shells(max_radius, num_radii, sample_density):
+    """Shell radii and sample counts of distributed_mc_radial_profile
+    (profile.cpp:93-128, 320-355)."""
+    radii = np.zeros(num_radii, np.float64)
+    counts = np.zeros(num_radii, np.uint64)
+    rc = _profile_lib().orc_mc_profile_shells(float(max_radius), int(num_radii),
+                                              float(sample_density), _p(radii), _p(counts))
+    if rc:
+        raise ValueError("invalid profile shells")
+    return radii, counts
+
+
+def mc_radial_profile(grid, center, max_radius, num_radii, sample_density, seed=0, dV_mode=0,
+                      volume_conversion=1.0, samples=False, nthreads=0):
+    """The oracle's Monte-Carlo radial profile of the grid's q around center:
+    the profile, and with samples=True every sample point (total, 4) and
+    nn8 value (total,) in sample order."""
+    L = _profile_lib()
+    total = int(mc_profile_shells(max_radius, num_radii, sample_density)[1].sum())
+    c = np.ascontiguousarray(center, np.float64)
+    prof = np.zeros(num_radii, np.float64)
+    pts = np.zeros((total, 4), np.float32) if samples else None
+    vals = np.zeros(total, np.float32) if samples else None
+    rc = L.orc_mc_radial_profile(grid.h, _p(c), float(max_radius), int(num_radii),
+                                 float(sample_density), int(seed), int(dV_mode),
+                                 float(volume_conversion), _p(prof), _p(pts), _p(vals), nthreads)
+    if rc:
+        raise ValueError("invalid profile arguments")
+    return (prof, pts, vals) if samples else prof

@@ -1797,4 +1797,134 @@ int orc_volumetric_slice(void* h, const orc_camera* c, double dV, float* out, in
   return 0;
 }
 
+// ---- Monte-Carlo radial profile -----------------------------------------
+// distributed_mc_radial_profile (profile.cpp:26-355) with the sampler of
+// random.cpp:28-86 drawing from a counter-based hash instead of the
+// reference's std::random_device-seeded std::mt19937: draw j of sample k is
+// the top 53 bits of mix(mix(seed ^ mix(k)) + j), mix = the SplitMix64 output
+// function (Steele, Lea, Flood 2014).
+static inline uint64_t prof_mix(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+static inline double prof_draw(uint64_t seed, uint64_t k, uint64_t j) {
+  const uint64_t h = prof_mix(prof_mix(seed ^ prof_mix(k)) + j);
+  return (double)(h >> 11) * (1.0 / 9007199254740992.0);
+}
+// Cube root from +, *, / and exact exponent scaling (so that it is the same
+// on any IEEE machine): u = m 2^(3q), m in [0.5, 4), eight Newton steps from 1.
+static inline double prof_cbrt(double u) {
+  if (!(u > 0.0)) return 0.0;
+  int e;
+  double m = std::frexp(u, &e);
+  int r = e % 3;
+  if (r < 0) r += 3;
+  m = std::ldexp(m, r);
+  e -= r;
+  double y = 1.0;
+  for (int i = 0; i < 8; ++i) y = (2.0 * y + m / (y * y)) / 3.0;
+  return std::ldexp(y, e / 3);
+}
+
+// profile.cpp:320-355 (shells) and 93-128 (generate_num_samples).
+static bool prof_shells(double R, int N, double density, std::vector<double>& rmin,
+                        std::vector<double>& rmax, std::vector<double>& vol,
+                        std::vector<uint64_t>& count) {
+  if (!(R > 0.0) || !std::isfinite(R) || N < 1 || N > (1 << 20) || !(density > 0.0) ||
+      !std::isfinite(density))
+    return false;
+  const unsigned n = (unsigned)N;
+  auto radius = [&](unsigned i) { return i * (R / n); };
+  rmin.resize(n); rmax.resize(n); vol.resize(n); count.resize(n);
+  for (unsigned i = 0; i < n; ++i) {
+    rmin[i] = i == 0 ? 0.0 : 0.5 * (radius(i - 1) + radius(i));
+    rmax[i] = 0.5 * (radius(i + 1) + radius(i));
+    vol[i] = 4. / 3 * M_PI * (rmax[i] * rmax[i] * rmax[i] - rmin[i] * rmin[i] * rmin[i]);
+  }
+  double expected = 0.0, sq = 0.0;
+  for (unsigned i = 0; i < n; ++i) expected += vol[i] * density;
+  for (unsigned i = 0; i < n; ++i) sq += vol[i] * vol[i];
+  const double norm = expected / sq;
+  uint64_t total = 0;
+  for (unsigned i = 0; i < n; ++i) {
+    const double want = norm * (vol[i] * vol[i]);
+    if (!(want < 1099511627776.0)) return false;
+    count[i] = (uint64_t)want;
+    if (count[i] == 0) count[i] = 1;
+    total += count[i];
+    if (total > 1099511627776ull) return false;
+  }
+  return true;
+}
+
+int orc_mc_profile_shells(double R, int N, double density, double* radii, uint64_t* counts) {
+  std::vector<double> a, b, v;
+  std::vector<uint64_t> c;
+  if (!prof_shells(R, N, density, a, b, v, c)) return 1;
+  for (int i = 0; i < N; ++i) {
+    if (radii) radii[i] = i * (R / (unsigned)N);
+    if (counts) counts[i] = c[i];
+  }
+  return 0;
+}
+
+// The profile: sample k (shells in order) uniform in its shell
+// (uniform_spherical_shell, random.cpp:67-86, with Marsaglia's surface point
+// of random.cpp:28-45: at most 64 attempts, then the pole), cast to float as
+// to_device_vector4 (cl_types.hpp:55-61); nn8 value summed per shell in
+// double in sample order (profile.cpp:212-225); times the effective dV of
+// apply_volume_factor (profile.cpp:236-256), mode 0 dV * conv, mode 1
+// (dV * conv) / (V * conv).
+int orc_mc_radial_profile(void* h, const double* center, double R, int N, double density,
+                          uint64_t seed, int mode, double conv, double* profile, float* pts,
+                          float* vals, int nthreads) {
+  Grid* g = (Grid*)h;
+  std::vector<double> rmin, rmax, vol;
+  std::vector<uint64_t> count;
+  if (!prof_shells(R, N, density, rmin, rmax, vol, count) || (mode != 0 && mode != 1)) return 1;
+  std::vector<uint64_t> first(N + 1, 0);
+  for (int i = 0; i < N; ++i) first[i + 1] = first[i] + count[i];
+  const uint64_t total = first[N];
+  std::vector<float> v(total);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < (int64_t)total; ++k) {
+    const int s = (int)(std::upper_bound(first.begin(), first.end(), (uint64_t)k) -
+                        first.begin()) - 1;
+    double x1 = 0.0, x2 = 0.0, r = 0.0;
+    for (int a = 0; a < 64; ++a) {
+      const double t1 = -1. + (1. - -1.) * prof_draw(seed, (uint64_t)k, 2 * a);
+      const double t2 = -1. + (1. - -1.) * prof_draw(seed, (uint64_t)k, 2 * a + 1);
+      const double rr = t1 * t1 + t2 * t2;
+      if (rr <= 1.) {
+        x1 = t1; x2 = t2; r = rr;
+        break;
+      }
+    }
+    const double sq = std::sqrt(1. - r);
+    const double p[3] = {2 * x1 * sq, 2 * x2 * sq, 1 - 2 * r};
+    const double u_min = rmin[s] * rmin[s] * rmin[s], u_max = rmax[s] * rmax[s] * rmax[s];
+    const double u = u_min + (u_max - u_min) * prof_draw(seed, (uint64_t)k, 128);
+    const double rad = prof_cbrt(u);
+    float q[3];
+    for (int j = 0; j < 3; ++j) q[j] = (float)(rad * p[j] + center[j]);
+    v[k] = nn8_value<float>(*g, q[0], q[1], q[2], nullptr);
+    if (pts) {
+      for (int j = 0; j < 3; ++j) pts[4 * k + j] = q[j];
+      pts[4 * k + 3] = 0.0f;
+    }
+    if (vals) vals[k] = v[k];
+  }
+  for (int s = 0; s < N; ++s) {
+    double sum = 0.0;
+    for (uint64_t k = first[s]; k < first[s + 1]; ++k) sum += (double)v[k];
+    const double dV = vol[s] / (double)count[s];
+    const double eff = mode == 0 ? dV * conv : (dV * conv) / (vol[s] * conv);
+    profile[s] = sum * eff;
+  }
+  return 0;
+}
+
 }  // extern "C"

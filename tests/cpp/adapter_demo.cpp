@@ -45,6 +45,10 @@ int main() {
     std::vector<float> slice;
     ilc::volumetric_slice(ctx, cam, 1.0, slice);
     for (float v : slice) sum += v;
+    std::vector<double> radii;
+    const auto prof = ilc::mc_radial_profile(ctx, {50.0, 50.0, 50.0}, 30.0, 6, 0.05, 3,
+                                             ILC_DV_MEAN, 1.0, &radii);
+    for (std::size_t i = 0; i < prof.size(); ++i) sum += prof[i] * 1e-6 + radii[i] * 1e-9;
     std::vector<float> krho, ku, kxe;
     for (uint32_t i : kept_index) {
       krho.push_back(rho[i]);
