@@ -138,6 +138,22 @@ def mc_profile_shells(max_radius, num_radii, sample_density):
     return radii, counts
 
 
+def mc_profile_points(center, max_radius, num_radii, sample_density, seed=0, first=0,
+                      count=None):
+    """Sample points first .. first + count - 1 of a Monte-Carlo radial profile
+    (ilc_mc_profile_points; host only), (count, 4) float32 with w = 0."""
+    if count is None:
+        count = int(mc_profile_shells(max_radius, num_radii, sample_density)[1].sum()) - first
+    c = np.ascontiguousarray(center, np.float64)
+    out = np.zeros((count, 4), np.float32)
+    st = _lib.load().ilc_mc_profile_points(_ptr(c), float(max_radius), int(num_radii),
+                                            float(sample_density), int(seed), int(first),
+                                            int(count), _ptr(out))
+    if st != _lib.ILC_OK:
+        raise IlcError(st, "invalid profile sample range or shells")
+    return out
+
+
 def camera_plane(cam):
     out = np.zeros(13, np.float32)
     st = _lib.load().ilc_camera_plane(ctypes.byref(cam), _ptr(out))

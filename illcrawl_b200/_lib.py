@@ -129,6 +129,7 @@ SIGNATURES = {
                                              _P, _int]),
     "ilc_arf_load": (_int, [_P, _P, _i32, _f32, _f32]),
     "ilc_mc_profile_shells": (_int, [_f64, _i32, _f64, _P, _P]),
+    "ilc_mc_profile_points": (_int, [_P, _f64, _i32, _f64, _u64, _u64, _u64, _P]),
     "ilc_mc_radial_profile": (_int, [_P, _P, _f64, _i32, _f64, _u64, _i32, _f64, _P, _P, _P]),
     "ilc_quantity_chandra_count_rate": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _P, _int]),
     "ilc_quantity_chandra_spectral_count_rate": (_int, [_P, _P, _P, _P, _u64, _f32, _f32, _f32,

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "ilc_internal.h"
+#include "ilc_random.cuh"
 
 struct ilc_ctx {
   ilc::Context c;
@@ -388,6 +389,7 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
 // arithmetic and summation order.
 struct ProfileShells {
   std::vector<double> radius, r_min, r_max, volume;
+  std::vector<double> u_min, u_max;     // uniform_spherical_shell's u range (random.cpp:67-74)
   std::vector<uint64_t> count, prefix;  // prefix: num_radii + 1 entries
 };
 
@@ -405,12 +407,16 @@ bool profile_shells(double max_radius, int32_t num_radii, double density, Profil
   S->r_min.resize(N);
   S->r_max.resize(N);
   S->volume.resize(N);
+  S->u_min.resize(N);
+  S->u_max.resize(N);
   for (unsigned i = 0; i < N; ++i) {
     S->radius[i] = radius(i);
     S->r_min[i] = i == 0 ? 0.0 : 0.5 * (radius(i - 1) + radius(i));
     S->r_max[i] = 0.5 * (radius(i + 1) + radius(i));
     const double a = S->r_min[i], b = S->r_max[i];
     S->volume[i] = 4. / 3 * M_PI * (b * b * b - a * a * a);
+    S->u_min[i] = a * a * a;
+    S->u_max[i] = b * b * b;
   }
   double expected = 0.0, sum_sq = 0.0;
   for (unsigned i = 0; i < N; ++i) expected += S->volume[i] * density;
@@ -1437,6 +1443,27 @@ ilc_status ilc_mc_profile_shells(double max_radius, int32_t num_radii, double sa
   return ILC_OK;
 }
 
+ilc_status ilc_mc_profile_points(const double center[3], double max_radius, int32_t num_radii,
+                                 double sample_density, uint64_t seed, uint64_t first,
+                                 uint64_t count, float* points) {
+  ProfileShells S;
+  if (!center || (count > 0 && !points) ||
+      !profile_shells(max_radius, num_radii, sample_density, &S))
+    return ILC_ERR_INVALID_ARGUMENT;
+  const uint64_t total = S.prefix[(size_t)num_radii];
+  if (first > total || count > total - first) return ILC_ERR_INVALID_ARGUMENT;
+  for (uint64_t k = 0; k < count; ++k) {
+    const uint64_t g = first + k;
+    const int s = find_shell(S.prefix.data(), num_radii, g);
+    const ShellPoint p = shell_sample(seed, g, S.u_min[s], S.u_max[s], center);
+    points[4 * k + 0] = p.x;
+    points[4 * k + 1] = p.y;
+    points[4 * k + 2] = p.z;
+    points[4 * k + 3] = 0.0f;
+  }
+  return ILC_OK;
+}
+
 ilc_status ilc_mc_radial_profile(ilc_ctx* h, const double center[3], double max_radius,
                                  int32_t num_radii, double sample_density, uint64_t seed,
                                  int32_t dV_mode, double volume_conversion, double* profile,
@@ -1461,9 +1488,8 @@ ilc_status ilc_mc_radial_profile(ilc_ctx* h, const double center[3], double max_
   double* t_umax = t_umin + N;
   for (uint32_t i = 0; i <= N; ++i) t_prefix[i] = S.prefix[i];
   for (uint32_t i = 0; i < N; ++i) {
-    // uniform_spherical_shell's u range (random.cpp:67-74)
-    t_umin[i] = S.r_min[i] * S.r_min[i] * S.r_min[i];
-    t_umax[i] = S.r_max[i] * S.r_max[i] * S.r_max[i];
+    t_umin[i] = S.u_min[i];
+    t_umax[i] = S.u_max[i];
   }
   // reduction segments: at most kProfileSegment consecutive samples of one shell
   std::vector<ulonglong2> segs;

@@ -35,12 +35,8 @@ __global__ void profile_points_kernel(const uint64_t* __restrict__ prefix, int n
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
        k += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t g = g0 + k;
-    int lo = 0, hi = n_shells;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (prefix[mid] <= g) lo = mid; else hi = mid;
-    }
-    const ShellPoint p = shell_sample(seed, g, u_min[lo], u_max[lo], c);
+    const int s = find_shell(prefix, n_shells, g);
+    const ShellPoint p = shell_sample(seed, g, u_min[s], u_max[s], c);
     pts[k] = make_float4(p.x, p.y, p.z, 0.0f);
   }
 }

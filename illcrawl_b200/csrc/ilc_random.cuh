@@ -56,6 +56,18 @@ __host__ __device__ __forceinline__ double cbrt_newton(double u) {
 // math::to_device_vector4 does (cl_types.hpp:55-61). Attempt a of the surface
 // draw uses draws 2a and 2a + 1; after 64 rejections (probability 2e-43) the
 // pole (0, 0, 1) is taken. The radius uses draw 128.
+// Shell of global sample g: the lo with prefix[lo] <= g < prefix[lo + 1]
+// (prefix: n_shells + 1 increasing entries from 0, g < prefix[n_shells]).
+__host__ __device__ __forceinline__ int find_shell(const uint64_t* prefix, int n_shells,
+                                                   uint64_t g) {
+  int lo = 0, hi = n_shells;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (prefix[mid] <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
 struct ShellPoint {
   float x, y, z;
 };

@@ -343,6 +343,14 @@ enum { ILC_DV_VOLUME = 0, ILC_DV_MEAN = 1 };
 ilc_status ilc_mc_profile_shells(double max_radius, int32_t num_radii, double sample_density,
                                  double* radii, uint64_t* counts);
 
+/* Sample points first .. first + count - 1 of that profile (4 floats each,
+ * w = 0), made on the host by the same code as the device's: for callers that
+ * evaluate the samples elsewhere or split them over processes (the
+ * reference's work_partitioner split of profile.cpp:156-177). Host only. */
+ilc_status ilc_mc_profile_points(const double center[3], double max_radius, int32_t num_radii,
+                                 double sample_density, uint64_t seed, uint64_t first,
+                                 uint64_t count, float* points);
+
 /* The profile of the particles' q (ilc_nn8_setup_particles) around center:
  * per shell, the nn8 values at its samples summed in double, times the
  * quantity's effective dV of apply_volume_factor (profile.cpp:236-256) with

@@ -70,7 +70,7 @@ def test_every_entry_point_rejects_a_null_context(cuda_lib):
     L = _lib.load()
     skip = {"ilc_create", "ilc_destroy", "ilc_camera_plane", "ilc_los_scale",
             "ilc_grid_build_noalloc", "ilc_fits_write_image",
-            "ilc_mc_profile_shells"}  # context-free by design
+            "ilc_mc_profile_shells", "ilc_mc_profile_points"}  # context-free by design
     checked = 0
     for name, (res, args) in _lib.SIGNATURES.items():
         if name in skip:

@@ -162,3 +162,31 @@ def test_constant_field_profile(oracle_mod, mode):
     vol = np.array([4. / 3 * math.pi * (b ** 3 - a ** 3) for a, b in zip(rmin, rmax)])
     want = np.full(10, 2.5) if mode == 1 else 2.5 * vol * 0.125
     assert np.allclose(prof, want, rtol=1e-6)
+
+
+@pytest.mark.parametrize("seed,R,N,density,first,count", [(99, 400.0, 12, 1e-4, 0, None),
+                                                          (3, 1000.0, 8, 1e-5, 5000, 20000),
+                                                          (2 ** 63 + 5, 50.0, 3, 0.2, 17, 1)])
+def test_library_sampler_matches_oracle(oracle_mod, cuda_lib, seed, R, N, density, first, count):
+    """The library's sampler source (host build of the code the device runs:
+    shell search, hashed draws, Marsaglia point, Newton cube root) makes the
+    oracle's sample points bit for bit."""
+    import illcrawl_b200 as ilc
+    from illcrawl_b200 import synthetic
+    c = synthetic.small_cells(2_000, seed=66)
+    g = oracle_mod.Grid(c.xyzq(c.rho))
+    center = (480.5, 510.25, 499.0)
+    _, opts, _ = oracle_mod.mc_radial_profile(g, center, R, N, density, seed=seed, samples=True)
+    total = opts.shape[0]
+    n = total - first if count is None else count
+    pts = ilc.mc_profile_points(center, R, N, density, seed=seed, first=first, count=n)
+    assert pts.shape == (n, 4)
+    assert np.array_equal(pts.view(np.uint32), opts[first:first + n].view(np.uint32))
+
+
+def test_library_sampler_rejects_out_of_range(cuda_lib):
+    import illcrawl_b200 as ilc
+    total = int(ilc.mc_profile_shells(100.0, 4, 0.01)[1].sum())
+    with pytest.raises(ilc.IlcError):
+        ilc.mc_profile_points((0, 0, 0), 100.0, 4, 0.01, first=total - 1, count=2)
+    assert ilc.mc_profile_points((0, 0, 0), 100.0, 4, 0.01, first=total, count=0).shape == (0, 4)
