@@ -12,6 +12,11 @@ benchmark. Names follow the reference's interfaces:
   :func:`mean_temperature` -- the quantity kernels of quantities.cl
 * :func:`load_gaunt_table` -- ``util::data_table_loader`` on gaunt_factor.dat
   (data_table_loader.hpp:39-97)
+* :meth:`Context.volumetric_slice`, :meth:`Context.volumetric_tomography`,
+  :meth:`Context.mc_radial_profile` -- the other nn8 consumers
+  (volumetric_slice.cpp, volumetric_tomography.cpp, profile.cpp);
+  :mod:`illcrawl_b200.distributed` splits them over processes as the
+  reference's distributed_* classes do
 
 All compute runs in ``libilcuda.so``; nothing here falls back to the CPU.
 """
