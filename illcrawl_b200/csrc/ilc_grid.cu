@@ -8,6 +8,7 @@
 // The stable sort gives the permutation boost::compute::sort_by_key gives, so
 // keys, permutation and cell ranges are bit-identical to the reference's.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -358,14 +359,14 @@ void spiral_table(int8_t out[8][125][3]) {
 // Allocation-free grid build.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// grid: code running while a CUDA graph is being captured (cudaMalloc is not a
-// capturable operation), real-time loops with a fixed memory budget, or hosts
-// whose allocator owns every device buffer. ilc_grid_build_noalloc builds the
-// same particle grid as ilc_nn8_setup_particles without any allocation: the
-// caller passes device buffers for the inputs and outputs, and the sort's
-// scratch space is this file-scope device array, sized for at most
-// ILC_NOALLOC_MAX_PARTICLES particles (about 16.5 MiB, held on every GPU that
-// loads the library until the process exits).
+// grid: real-time loops with a fixed memory budget, or hosts whose allocator
+// owns every device buffer. ilc_grid_build_noalloc builds the same particle
+// grid as ilc_nn8_setup_particles without any allocation: the caller passes
+// device buffers for the inputs and outputs, and the sort's scratch space is
+// this file-scope device array, sized for at most ILC_NOALLOC_MAX_PARTICLES
+// particles (about 16.5 MiB, held on every GPU that loads the library until
+// the process exits). The grid parameters are computed on the host from the
+// bounding box, so the call waits on its stream before it returns.
 // ---------------------------------------------------------------------------
 namespace ilc {
 namespace {
@@ -386,8 +387,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 // Device address of g_noalloc_scratch per device, looked up once per device
 // with that device current (in host code the symbol is only a host-side
 // stand-in for the array, not a device address).
+// Every thread that looks it up stores the same value, so relaxed atomics
+// suffice to make concurrent first calls well defined.
 constexpr int kMaxDevices = 64;
-static void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+static std::atomic<void*> g_noalloc_ptr[kMaxDevices];
 
 }  // namespace
 }  // namespace ilc
@@ -403,12 +406,12 @@ extern "C" ilc_status ilc_grid_build_noalloc(const float* particles, uint64_t n,
   if (n > kNoAllocMax) return ILC_ERR_INVALID_ARGUMENT;  // beyond the scratch array
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ILC_ERR_CUDA;
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ILC_ERR_CUDA;
-    g_noalloc_ptr[dev] = p;
+  void* sp = g_noalloc_ptr[dev].load(std::memory_order_relaxed);
+  if (!sp) {
+    if (cudaGetSymbolAddress(&sp, g_noalloc_scratch) != cudaSuccess || !sp) return ILC_ERR_CUDA;
+    g_noalloc_ptr[dev].store(sp, std::memory_order_relaxed);
   }
-  unsigned char* s = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  unsigned char* s = static_cast<unsigned char*>(sp);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const float4* in = reinterpret_cast<const float4*>(particles);
   unsigned* acc = reinterpret_cast<unsigned*>(s);

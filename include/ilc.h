@@ -277,6 +277,20 @@ ilc_status ilc_render_record(ilc_ctx* ctx, const ilc_camera* cam, double z_range
                              int32_t* n_steps, int64_t capacity, int steps_on_device,
                              float* image, int is_device, ilc_render_stats* stats);
 
+/* ilc_render_adaptive that also writes each ray's work counters: ray
+ * k = iy * num_pix_x + ix gets ray_stats[4k .. 4k+3] = (RKF steps taken,
+ * steps accepted, grid cells visited, candidate particles tested), summed
+ * over the 4 integrand points of every step as the oracle's search counters
+ * count them (volumetric_nn8_reconstruction.cl:157-203 visits a cell and
+ * tests every particle in it). They give each ray's algorithmic bytes
+ * 8 cells + 16 candidates + 24 steps + 4. Runs the one-block-per-tile kernel;
+ * the image equals ilc_render_adaptive's. ray_stats follows is_device. No
+ * reference counterpart as an entry point. */
+ilc_status ilc_render_ray_stats(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                                ilc_tolerance tol, int32_t controller,
+                                const ilc_los_scaling* scaling, float* image,
+                                uint64_t* ray_stats, int is_device, ilc_render_stats* stats);
+
 /* Frozen per-ray step sequence: ray k replays step_sizes[k * capacity + i],
  * i < n_steps[k], every step accepted (I += delta4 of integration.cl:63-79,
  * k1 carried), from z = 0. Replaying a recorded adaptive sequence gives the
@@ -521,23 +535,25 @@ ilc_status ilc_autotune_render(ilc_ctx* ctx, const ilc_camera* cam, double z_ran
                                int32_t* best_occupancy, float* times_ms);
 
 /* Allocation-free grid build, for callers that cannot allocate device memory
- * when they need a grid (for example while a CUDA graph is being captured, in
- * a real-time loop with a fixed memory budget, or under a host allocator that
- * owns all device buffers). No counterpart in the reference. It builds the
- * same grid as ilc_nn8_setup_particles into caller-owned device buffers:
- * particles (n float4), sorted_particles (n float4), cells (cells_capacity
- * int2), sorted_to_unsorted (n uint32), all on the current device; desc
- * receives the grid parameters (also when cells_capacity is too small, so the
- * caller can size the cells buffer and call again). It allocates nothing: the
- * sort's scratch is a fixed device array inside the library, sized for at
- * most ILC_NOALLOC_MAX_PARTICLES particles (about 16.5 MiB per GPU that loads
- * the library, held until the process exits); larger n is rejected with
- * ILC_ERR_INVALID_ARGUMENT. The first call on a device looks the array's
- * device address up once, so make that first call before any stream capture.
- * Every call shares the one scratch array: calls whose work overlaps on the
- * GPU (different streams or host threads at the same time) race. Work is
- * issued on `stream` (a cudaStream_t, NULL = default stream) and has finished
- * when the call returns. */
+ * when they need a grid (for example a real-time loop with a fixed device
+ * memory budget, or a host whose own allocator owns every device buffer and
+ * forbids allocations behind its back). No counterpart in the reference. It
+ * builds the same grid as ilc_nn8_setup_particles into caller-owned device
+ * buffers: particles (n float4), sorted_particles (n float4), cells
+ * (cells_capacity int2), sorted_to_unsorted (n uint32), all on the current
+ * device; desc receives the grid parameters (also when cells_capacity is too
+ * small, so the caller can size the cells buffer and call again). It
+ * allocates nothing: the sort's scratch is a fixed device array inside the
+ * library, sized for at most ILC_NOALLOC_MAX_PARTICLES particles (about
+ * 16.5 MiB per GPU that loads the library, held until the process exits);
+ * larger n is rejected with ILC_ERR_INVALID_ARGUMENT. The first call on a
+ * device looks the array's device address up once, so make that first call
+ * before any stream capture. Every call shares the one scratch array: calls
+ * whose work overlaps on the GPU (different streams or host threads at the
+ * same time) race. Work is issued on `stream` (a cudaStream_t, NULL = default
+ * stream); the call waits on that stream twice (for the bounding box, which
+ * the grid parameters are computed from on the host, and for the final
+ * status), so its work has finished when it returns. */
 #define ILC_NOALLOC_MAX_PARTICLES 1048576
 ilc_status ilc_grid_build_noalloc(const float* particles, uint64_t n, float* sorted_particles,
                                   int32_t* cells, uint64_t cells_capacity,

@@ -2,10 +2,11 @@
 as the regular entry point (ilc_nn8_setup_particles + ilc_grid_export).
 
 It serves callers that cannot allocate device memory where they need a grid
-(inside CUDA graph capture, fixed-budget real-time loops, hosts whose
-allocator owns the device memory): the test owns every device buffer and the
-entry point only uses its fixed internal scratch array. Two calls in a row
-check that the shared scratch left by one call does not leak into the next.
+(fixed-budget real-time loops, hosts whose allocator owns the device memory):
+the test owns every device buffer and the entry point only uses its fixed
+internal scratch array. Two calls in a row check that the shared scratch left
+by one call does not leak into the next, and a build of exactly
+ILC_NOALLOC_MAX_PARTICLES particles fills every region of the scratch array.
 This file is collected last, so a run that stops at the first failure has
 already run every other test."""
 import ctypes
@@ -58,6 +59,26 @@ def test_noalloc_grid_matches_regular_entry_point_twice(ctx):
         assert np.array_equal(cells, rcells)
         assert np.array_equal(s2u, rs2u)
         assert np.array_equal(srt.view(np.uint32), rsrt.view(np.uint32))
+
+
+def test_noalloc_grid_at_its_maximum_size(ctx):
+    """n = ILC_NOALLOC_MAX_PARTICLES: all 512 sort tiles and the whole key,
+    value and histogram regions of the scratch array are in use."""
+    import torch
+    from illcrawl_b200 import synthetic
+    lib = ctx.L
+    n = 1 << 20
+    c = synthetic.small_cells(n, seed=63)
+    pts = c.xyzq(c.rho)
+    mn, cs, nc, cells, s2u, srt = _noalloc_build(lib, torch, pts)
+    ctx.setup_particles(pts)
+    d = ctx.grid_describe()
+    rcells, rs2u, rsrt = ctx.grid_export()
+    assert np.array_equal(mn, d["min_corner"]) and np.array_equal(cs, d["cell_sizes"])
+    assert np.array_equal(nc, d["num_cells"])
+    assert np.array_equal(cells, rcells)
+    assert np.array_equal(s2u, rs2u)
+    assert np.array_equal(srt.view(np.uint32), rsrt.view(np.uint32))
 
 
 def test_noalloc_rejects_more_than_its_maximum(ctx):
