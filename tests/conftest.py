@@ -49,3 +49,22 @@ def random_queries(n, lo, hi, seed):
     q = np.zeros((n, 4), np.float32)
     q[:, :3] = (lo + rng.random((n, 3)) * (hi - lo)).astype(np.float32)
     return q
+
+
+def reference_arf():
+    """The reference's ARF (chandra.cpp arf_data[0:1024]) from the golden
+    fixture made by tests/golden/make_golden.py: (float32 table, x_min, dx)."""
+    path = os.path.join(ROOT, "tests", "golden", "chandra_arf.txt")
+    x0 = dx = None
+    bits = []
+    for line in open(path):
+        if line.startswith("#"):
+            continue
+        k = line.split()
+        if k[0] == "x_min":
+            x0 = float(k[1])
+        elif k[0] == "dx":
+            dx = float(k[1])
+        else:
+            bits.append(int(k[0], 16))
+    return np.array(bits, np.uint32).view(np.float32), x0, dx

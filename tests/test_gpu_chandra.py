@@ -12,6 +12,8 @@ and of maps and spectra rendered from them:
 import numpy as np
 import pytest
 
+from conftest import reference_arf
+
 from test_gpu_parity import same_bits
 
 pytestmark = pytest.mark.gpu
@@ -20,8 +22,14 @@ Z, DL = 0.2, 978500.0
 X0, DX = 0.105322271585, 0.010644
 
 
-@pytest.fixture(scope="module")
-def arf():
+@pytest.fixture(scope="module", params=["reference", "synthetic"])
+def arf(request):
+    """The reference's own ARF (golden fixture from chandra.cpp) and a seeded
+    stand-in on the same energy grid."""
+    if request.param == "reference":
+        table, x0, dx = reference_arf()
+        assert (x0, dx) == (X0, DX)
+        return table
     from illcrawl_b200 import synthetic
     return synthetic.synthetic_arf()
 

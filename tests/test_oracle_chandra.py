@@ -12,6 +12,8 @@
 import numpy as np
 import pytest
 
+from conftest import reference_arf
+
 Z, DL = 0.2, 978500.0
 X0, DX = 0.105322271585, 0.010644
 
@@ -37,8 +39,14 @@ def _arf_np(arf, x):
     return (f(1) - a) * t0 + a * t1
 
 
-@pytest.fixture(scope="module")
-def arf():
+@pytest.fixture(scope="module", params=["reference", "synthetic"])
+def arf(request):
+    """The reference's own ARF (golden fixture from chandra.cpp) and a seeded
+    stand-in on the same energy grid."""
+    if request.param == "reference":
+        table, x0, dx = reference_arf()
+        assert (x0, dx) == (X0, DX)
+        return table
     from illcrawl_b200 import synthetic
     return synthetic.synthetic_arf()
 
@@ -142,3 +150,15 @@ def test_photon_flux_is_flux_over_energy(oracle_mod, gaunt_table):
     ef = oracle_mod.xray_band(gaunt_table, rho, u, xe, Z, DL, 0.5, 7.0, 100, precision=1)
     mean_e = ef.astype(np.float64) * 1e-4 / pf   # keV per photon at the source
     assert np.all(mean_e > (1 + Z) * 0.5) and np.all(mean_e < (1 + Z) * 7.0)
+
+
+def test_reference_arf_fixture():
+    """The fixture holds chandra.cpp's table as the compiler makes it: 1024
+    float32 entries from x_min 0.105322271585 keV in steps of 0.010644 keV,
+    the first of them the literals 7.977484415e-07f and 3.577559582e-08f."""
+    table, x0, dx = reference_arf()
+    assert table.dtype == np.float32 and table.shape == (1024,)
+    assert (x0, dx) == (0.105322271585, 0.010644)
+    assert table[0] == np.float32(7.977484415e-07) and table[1] == np.float32(3.577559582e-08)
+    assert np.all(np.isfinite(table)) and np.all(table > 0)
+    assert 400.0 < table.max() < 450.0   # peak effective area in cm^2
