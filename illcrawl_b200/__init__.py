@@ -577,6 +577,21 @@ class Context:
                                             ctypes.byref(st)))
         return img, hs, n, st.as_dict()
 
+    def render_ray_stats(self, cam, z_range, rel_tol=1e-3, abs_tol=0.0,
+                         controller=CONTROLLER_FP64, scaling=None):
+        """Adaptive render plus each ray's work counters (ilc_render_ray_stats):
+        (image, counters (rays, 4) uint64 = steps, accepted, cells visited,
+        candidates tested, stats)."""
+        img = self._image(cam, False)
+        rays = cam.num_pix_x * cam.num_pix_y
+        rs = np.zeros((rays, 4), np.uint64)
+        st = RenderStats()
+        sc = None if scaling is None else ctypes.byref(scaling)
+        self.check(self.L.ilc_render_ray_stats(self.h, ctypes.byref(cam), float(z_range),
+                                               Tolerance(abs_tol, rel_tol), controller, sc,
+                                               _ptr(img), _ptr(rs), 0, ctypes.byref(st)))
+        return img, rs, st.as_dict()
+
     def render_frozen(self, cam, z_range, step_sizes, n_steps, scaling=None):
         """Replays per-ray step sequences (rays x capacity), all accepted."""
         hs = np.ascontiguousarray(step_sizes, np.float32)

@@ -114,6 +114,7 @@ SIGNATURES = {
     "ilc_render_fixed": (_int, [_P, _P, _f64, _i64, _P, _P, _int, _P]),
     "ilc_render_record": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _P, _i64, _int, _P, _int, _P]),
     "ilc_render_frozen": (_int, [_P, _P, _f64, _P, _P, _i64, _int, _P, _P, _int, _P]),
+    "ilc_render_ray_stats": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _P, _P, _int, _P]),
     "ilc_los_scale": (_f32, [_P, _f64, _P]),
     "ilc_project_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
                                      _f64, Tolerance, _i32, _P, _P, _int, _P]),

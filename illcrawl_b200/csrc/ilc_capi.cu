@@ -306,6 +306,7 @@ struct StepArrays {
   float* rec_h = nullptr;
   int32_t* rec_n = nullptr;
   int64_t cap = 0;
+  uint64_t* ray_stats = nullptr;  // per-ray statistics (device)
 };
 
 ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_tolerance tol,
@@ -342,13 +343,14 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
   a.rec_h = sa.rec_h;
   a.rec_n = sa.rec_n;
   a.rec_cap = sa.cap;
+  a.ray_stats = sa.ray_stats;
   const size_t bytes = (size_t)a.nx * (size_t)a.ny * 4;
   void* dimg = nullptr;
   ILC_CUDA(c, out_ptr(c.out_a, image, bytes, is_device, &dimg), "image buffer");
   a.out = static_cast<float*>(dimg);
   float ms = 0.0f;
   if (c.render_engine == ILC_ENGINE_PERSISTENT && fixed_steps <= 0 &&
-      controller == ILC_CONTROLLER_FP64 && !sa.replay_h && !sa.rec_h) {
+      controller == ILC_CONTROLLER_FP64 && !sa.replay_h && !sa.rec_h && !sa.ray_stats) {
     // one job through the persistent work-queue kernel, values = particle q
     ilc_job j{};
     j.camera = *cam;
@@ -895,6 +897,26 @@ ilc_status ilc_render_record(ilc_ctx* h, const ilc_camera* cam, double z_range,
   ILC_CUDA(c, finish_out(c, step_sizes, dh, rays * (uint64_t)capacity * 4, steps_on_device),
            "step buffer D2H");
   ILC_CUDA(c, finish_out(c, n_steps, dn, rays * 4, steps_on_device), "step counts D2H");
+  return st;
+}
+
+ilc_status ilc_render_ray_stats(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                                ilc_tolerance tol, int32_t controller,
+                                const ilc_los_scaling* scaling, float* image,
+                                uint64_t* ray_stats, int is_device, ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!camera_ok(cam) || !ray_stats)
+    return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid per-ray statistics arguments");
+  const uint64_t bytes = (uint64_t)cam->num_pix_x * (uint64_t)cam->num_pix_y * 32;
+  void* dr = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_b, ray_stats, bytes, is_device, &dr), "ray statistics buffer");
+  StepArrays sa;
+  sa.ray_stats = static_cast<uint64_t*>(dr);
+  ilc_status st = render_common(c, cam, z_range, tol, controller, 0, scaling, image, is_device,
+                                stats, sa);
+  ILC_CUDA(c, finish_out(c, ray_stats, dr, bytes, is_device), "ray statistics D2H");
   return st;
 }
 

@@ -202,6 +202,7 @@ struct RenderArgs {
   int64_t rec_cap = 0;
   const float* replay_h = nullptr;    // frozen replay: per-ray step sizes (rec_cap each)
   const int32_t* replay_n = nullptr;  // frozen replay: steps per ray
+  uint64_t* ray_stats = nullptr;      // optional: per ray (steps, accepted, cells, candidates)
 };
 
 // Adjoint of the X-ray band map (ilc_adjoint.cu).

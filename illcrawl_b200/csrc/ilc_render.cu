@@ -55,6 +55,7 @@ struct RenderK {
   float scale;
   int apply_scale;
   float* out;
+  uint64_t* ray_stats;  // optional: per ray (steps, accepted, cells visited, candidates)
 };
 
 // Pixel tiling: a block of 128 threads covers 16 x 8 pixels; each warp an
@@ -157,6 +158,13 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
     }
   }
   if (active) a.out[(size_t)iy * a.cam.nx + ix] = a.apply_scale ? I * a.scale : I;
+  if (active && a.ray_stats) {
+    uint64_t* r = a.ray_stats + 4 * ((size_t)iy * a.cam.nx + ix);
+    r[0] = steps;
+    r[1] = acc;
+    r[2] = ws.cells;
+    r[3] = ws.cands;
+  }
   if (at_limit) atomicOr(flags, FLAG_STEP_LIMIT);
   // warp-aggregated statistics
   unsigned long long c = ws.cells, k = ws.cands, st = steps, ac = acc, mx = steps,
@@ -210,6 +218,7 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   k.scale = a.scale;
   k.apply_scale = a.apply_scale ? 1 : 0;
   k.out = a.out;
+  k.ray_stats = a.ray_stats;
   const GridView g = make_grid_view(c);
   const int tile_rows = (a.ny + kTileY - 1) / kTileY;
   dim3 grid((a.nx + kTileX - 1) / kTileX, (tile_rows + k.row_stride - 1) / k.row_stride);
