@@ -32,3 +32,48 @@ def test_measured_traffic_only_for_its_workload():
     assert bench.measured_traffic(args) is None
     bench.NX = 1024
     assert bench.measured_traffic(argparse.Namespace(engine="grid")) is None
+
+
+def test_both_arms_print_the_same_config():
+    sys.path.insert(0, ROOT)
+    import bench
+    bench.NX = bench.NY = 1024
+    bench.Z_START, bench.DEPTH = 0.0, bench.BOX
+    a, b = bench.workload_config(1), bench.workload_config(1)
+    assert a == b and a["cells"] == 4194304 and a["image"] == [1024, 1024]
+    assert a["rel_tol"] == 1e-3 and a["controller"] == "fp64"
+
+
+def test_accuracy_sample_is_the_bytes_file_sample():
+    sys.path.insert(0, ROOT)
+    import json
+    import numpy as np
+    import bench
+    bench.NX = bench.NY = 1024
+    d = json.load(open(os.path.join(ROOT, "baseline", "bytes_cfg1.json")))
+    assert np.array_equal(bench.sample_pixels(), [r["pixel"] for r in d["rays"]])
+    for r in d["rays"]:
+        assert r["bytes"] == 8 * r["cells_visited"] + 16 * r["candidates"] + 24 * r["steps"] + 4
+    assert abs(d["mean_bytes_per_ray"] - np.mean([r["bytes"] for r in d["rays"]])) < 1e-6
+
+
+def test_reference_arm_reports_the_work_it_did(capsys):
+    """Every step renders REF_SAMPLE rays on the oracle; ms_per_step is that
+    step's time and value the rate of those rays."""
+    sys.path.insert(0, ROOT)
+    import argparse
+    import json
+    import bench
+    bench.NX = bench.NY = 1024
+    bench.Z_START, bench.DEPTH = 0.0, bench.BOX
+    old = bench.REF_SAMPLE
+    bench.REF_SAMPLE = 8
+    try:
+        bench.run_reference(argparse.Namespace(steps=2, warmup=0), 0, 1)
+    finally:
+        bench.REF_SAMPLE = old
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["steps"] == 2
+    assert abs(line["value"] - 8 / (line["ms_per_step"] * 1e-3) / 1e6) < 1e-12
+    assert line["config"] == bench.workload_config(1)
+    assert line["full_image_estimate"]["seconds"] > line["ms_per_step"] * 1e-3
