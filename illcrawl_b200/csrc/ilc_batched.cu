@@ -164,7 +164,10 @@ __device__ __forceinline__ float channel_step(float Ic, float k1c, float e0, flo
   return (float)((double)Ic + d4);
 }
 
-template <bool kMulti, int kMinBlocks>
+// kMulti: V > 1 channels from the table. kOwnVal (V = 1 without a channel
+// table): the slots carry the particles' own q, as the render kernel's walk
+// does, so no value is looked up by index afterwards.
+template <bool kMulti, int kMinBlocks, bool kOwnVal>
 __global__ void __launch_bounds__(kBThreads, kMinBlocks)
 batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
                uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
@@ -232,13 +235,20 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
       if (go) {
         Step4 s;
         s4_bind(s, slot_mem);
-        nn8_walk_step4<true>(g, spiral, o[0], o[1], o[2], lx, ly, lz, pts, s, ws);
+        nn8_walk_step4<!kOwnVal>(g, spiral, o[0], o[1], o[2], lx, ly, lz, pts, s, ws);
         if (!kMulti) {
           float e[4];
-          e[0] = value1<0>(s, a.chan, g.parts);
-          e[1] = value1<1>(s, a.chan, g.parts);
-          e[2] = value1<2>(s, a.chan, g.parts);
-          e[3] = value1<3>(s, a.chan, g.parts);
+          if (kOwnVal) {
+            e[0] = s4_finalize<0>(s);
+            e[1] = s4_finalize<1>(s);
+            e[2] = s4_finalize<2>(s);
+            e[3] = s4_finalize<3>(s);
+          } else {
+            e[0] = value1<0>(s, a.chan, g.parts);
+            e[1] = value1<1>(s, a.chan, g.parts);
+            e[2] = value1<2>(s, a.chan, g.parts);
+            e[3] = value1<3>(s, a.chan, g.parts);
+          }
           const float zb = z;
           rkf_advance_fp64(I, z, h, k1, a.atol, a.rtol, len, e, kEps, kHmin, kHmax, pts);
           ++rs;
@@ -453,7 +463,8 @@ template <bool kMulti, int kMinBlocks>
 int persistent_blocks(const Context& c) {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_kernel<kMulti, kMinBlocks>,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+                                                batched_kernel<kMulti, kMinBlocks, false>,
                                                 kBThreads, 0);
   if (sms <= 0) sms = 148;
   if (per_sm <= 0) per_sm = 1;
@@ -463,7 +474,14 @@ int persistent_blocks(const Context& c) {
 template <bool kMulti, int kMinBlocks>
 cudaError_t launch_variant(Context& c, const BatchK& k, const GridView& g, int blocks) {
   unsigned long long* stats = reinterpret_cast<unsigned long long*>(c.flags.as<char>() + 64);
-  batched_kernel<kMulti, kMinBlocks><<<blocks, kBThreads, 0, c.stream>>>(
+  if constexpr (!kMulti) {
+    if (!k.chan) {
+      batched_kernel<false, kMinBlocks, true><<<blocks, kBThreads, 0, c.stream>>>(
+          k, g, c.spiral.as<char4>(), c.flags.as<uint32_t>(), stats);
+      return cudaGetLastError();
+    }
+  }
+  batched_kernel<kMulti, kMinBlocks, false><<<blocks, kBThreads, 0, c.stream>>>(
       k, g, c.spiral.as<char4>(), c.flags.as<uint32_t>(), stats);
   return cudaGetLastError();
 }

@@ -165,6 +165,30 @@ __device__ __forceinline__ void test_candidate(Step4& s, float thr[4], const flo
   cand_insert<kIdx>(s, thr, d2, P, p);
 }
 
+// With a shared x/y part, every point's squared distance is fl(fxy + fz^2)
+// >= fxy (rounding is monotone and fz^2 >= 0), so a candidate whose fxy
+// exceeds the largest threshold thrmax cannot be inserted for any point.
+// thrmax may be stale (larger than the current thresholds): the test only
+// skips work that could not insert.
+template <bool kSharedXY, bool kIdx>
+__device__ __forceinline__ void test_candidate_xy(Step4& s, float thr[4], float thrmax,
+                                                  const float4& P, int p) {
+  if (kSharedXY) {
+    const float fx = P.x - s.qx[0], fy = P.y - s.qy[0];
+    const float fxy = fx * fx + fy * fy;
+    if (fxy > thrmax) return;
+    float d2[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float fz = P.z - s.qz[j];
+      d2[j] = fxy + fz * fz;
+    }
+    cand_insert<kIdx>(s, thr, d2, P, p);
+  } else {
+    test_candidate<false, kIdx>(s, thr, P, p);
+  }
+}
+
 // Cells with more candidates than this are scanned through their sub-box codes.
 constexpr int kPruneMin = 16;
 
@@ -259,6 +283,9 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     if ((unsigned)ix >= (unsigned)g.n0 || (unsigned)iy >= (unsigned)g.n1 ||
         (unsigned)iz >= (unsigned)g.n2)
       continue;
+    // largest insertion threshold of the points still walking, fixed for
+    // this cell (thresholds only shrink, so it stays an upper bound)
+    const float thrmax = fmaxf(fmaxf(thr[0], thr[1]), fmaxf(thr[2], thr[3]));
     // ix + iy nx + iz nx ny, in 32 bits (the grid build rejects 2^32 cells or more)
     const uint32_t key = (uint32_t)ix + (uint32_t)g.n0 * ((uint32_t)iy + (uint32_t)g.n1 * (uint32_t)iz);
     const int2 be = __ldg(&g.cells[key]);
@@ -297,7 +324,7 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
         while (hits) {
           const int p = pw + __ffs(hits) - 1;
           hits &= hits - 1;
-          test_candidate<kSharedXY, kIdx>(s, thr, __ldg(&g.parts[p]), p);
+          test_candidate_xy<kSharedXY, kIdx>(s, thr, thrmax, __ldg(&g.parts[p]), p);
         }
       }
       continue;
@@ -305,28 +332,20 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     float4 P = __ldg(&g.parts[be.x]);
     for (int p = be.x; p < be.y; ++p) {
       const float4 N = (p + 1 < be.y) ? __ldg(&g.parts[p + 1]) : P;  // prefetch
-      test_candidate<kSharedXY, kIdx>(s, thr, P, p);
+      test_candidate_xy<kSharedXY, kIdx>(s, thr, thrmax, P, p);
       P = N;
     }
   }
 }
 
-// Cell and subcell of a point (volumetric_nn8_reconstruction.cl:129-155).
-__device__ __forceinline__ void locate(const GridView& g, float qx, float qy, float qz, int& cx,
-                                       int& cy, int& cz, int& sub) {
-  cx = clamp_cell(to_int_sat(floorf((qx - g.min0) / g.cs0)));
-  cy = clamp_cell(to_int_sat(floorf((qy - g.min1) / g.cs1)));
-  cz = clamp_cell(to_int_sat(floorf((qz - g.min2) / g.cs2)));
-  const float mx = g.min0 + (float)cx * g.cs0;
-  const float my = g.min1 + (float)cy * g.cs1;
-  const float mz = g.min2 + (float)cz * g.cs2;
-  int sx = to_int_sat(floorf((qx - mx) / g.half0));
-  int sy = to_int_sat(floorf((qy - my) / g.half1));
-  int sz = to_int_sat(floorf((qz - mz) / g.half2));
-  sx = min(max(sx, 0), 1);
-  sy = min(max(sy, 0), 1);
-  sz = min(max(sz, 0), 1);
-  sub = sx + 2 * sy + 4 * sz;
+// Cell index and subcell half (0/1) of a point along one axis
+// (volumetric_nn8_reconstruction.cl:129-155, one component).
+__device__ __forceinline__ void locate_axis(float q, float mn, float cs, float half, int& c,
+                                            int& sh) {
+  c = clamp_cell(to_int_sat(floorf((q - mn) / cs)));
+  const float m = mn + (float)c * cs;
+  const int si = to_int_sat(floorf((q - m) / half));
+  sh = min(max(si, 0), 1);
 }
 
 // nn8 walk of the 4 points of one step; the slots are left in s.
@@ -341,7 +360,25 @@ __device__ __forceinline__ void nn8_walk_step4(const GridView& g,
     s.qx[j] = px + zq[j] * lx;
     s.qy[j] = py + zq[j] * ly;
     s.qz[j] = pz + zq[j] * lz;
-    locate(g, s.qx[j], s.qy[j], s.qz[j], cx[j], cy[j], cz[j], sb[j]);
+  }
+  const bool shared_xy = s.qx[0] == s.qx[1] && s.qx[0] == s.qx[2] && s.qx[0] == s.qx[3] &&
+                         s.qy[0] == s.qy[1] && s.qy[0] == s.qy[2] && s.qy[0] == s.qy[3];
+  // points with bit-identical x and y (a view along z) share their x/y cell
+  // and subcell: located once
+  int cx0, sx0, cy0, sy0;
+  locate_axis(s.qx[0], g.min0, g.cs0, g.half0, cx0, sx0);
+  locate_axis(s.qy[0], g.min1, g.cs1, g.half1, cy0, sy0);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    int sx = sx0, sy = sy0, sz;
+    cx[j] = cx0;
+    cy[j] = cy0;
+    if (j > 0 && !shared_xy) {
+      locate_axis(s.qx[j], g.min0, g.cs0, g.half0, cx[j], sx);
+      locate_axis(s.qy[j], g.min1, g.cs1, g.half1, cy[j], sy);
+    }
+    locate_axis(s.qz[j], g.min2, g.cs2, g.half2, cz[j], sz);
+    sb[j] = sx + 2 * sy + 4 * sz;
   }
   s.crad = g.cell_radius;
   const float empty = kIdx ? __int_as_float(-1) : 0.0f;  // empty slots carry index -1
@@ -349,8 +386,6 @@ __device__ __forceinline__ void nn8_walk_step4(const GridView& g,
   s4_init<1>(s, empty);
   s4_init<2>(s, empty);
   s4_init<3>(s, empty);
-  const bool shared_xy = s.qx[0] == s.qx[1] && s.qx[0] == s.qx[2] && s.qx[0] == s.qx[3] &&
-                         s.qy[0] == s.qy[1] && s.qy[0] == s.qy[2] && s.qy[0] == s.qy[3];
   unsigned todo = 0xFu;
   while (todo) {
     const int j0 = __ffs(todo) - 1;
