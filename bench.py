@@ -464,6 +464,11 @@ def adjoint_leg(ctx, ilc, cells, args):
                                       rel_tol=REL_TOL, e_min=E_MIN, e_max=E_MAX,
                                       num_samples=NUM_SAMPLES)
     out = {"workload": "512^2 band map, 4,194,304 cells, target log T + GRF(0.1, 200 kpc)"}
+    # the fastest forward of the same map: the persistent work-queue kernel
+    _, fst = ctx.project_xray_flux(xyz4, cells.rho, cells.u, cells.xe, cam, DEPTH,
+                                   rel_tol=REL_TOL, e_min=E_MIN, e_max=E_MAX,
+                                   num_samples=NUM_SAMPLES)
+    out["forward_persistent_ms"] = fst["kernel_ms"]
     for name, mode in (("checkpoint", ilc._lib.ADJOINT_CHECKPOINT),
                        ("recompute", ilc._lib.ADJOINT_RECOMPUTE)):
         _, _, _, st = ctx.adjoint_xray_flux(xyz4, cells.rho, cells.u, cells.xe, cam, DEPTH,
@@ -472,6 +477,7 @@ def adjoint_leg(ctx, ilc, cells, args):
         out[name] = {"forward_ms": st["forward_ms"], "adjoint_ms": st["adjoint_ms"],
                      "quantity_ms": st["quantity_ms"],
                      "adjoint_over_forward": st["adjoint_ms"] / st["forward_ms"],
+                     "adjoint_over_persistent_forward": st["adjoint_ms"] / fst["kernel_ms"],
                      "loss": st["loss"]}
     return out
 
@@ -670,6 +676,128 @@ def run_ours(args, rank, world, local_rank):
     ctx.close()
 
 
+def run_scale(args):
+    """--config 4: the scale workload on one GPU. 67,108,864 seeded cells in an
+    8 Mpc cube (two NFW halos, 3:1, 1.5 Mpc apart, 10 % background):
+
+    * per-cell band flux + grid build, device-timed; the grid checked against
+      the oracle's (cell ranges, sorted->original map and sorted particles, bit
+      for bit);
+    * the 2048^2 0.5-7 keV band map along z through the 8 Mpc box (adaptive,
+      rtol 1e-3, FP64 controller), device-timed, with the clocks sampled;
+    * its adjoint with per-ray step checkpoints, in bands of pixel rows that
+      fit a 64 GiB checkpoint budget, against a target that is the map times
+      a seeded per-pixel lognormal (sigma 0.1);
+    * a 64-bin spectrum (log bins 0.3-10 keV) over a 512^2 aperture (4 Mpc
+      camera, circular aperture of radius 2 Mpc through the whole box) in one
+      batched launch."""
+    import torch
+    import oracle
+    import illcrawl_b200 as ilc
+    from illcrawl_b200 import synthetic
+    box, side = 8000.0, 2048
+    t0 = time.perf_counter()
+    cells = synthetic.scale_cells()
+    t_gen = time.perf_counter() - t0
+    n = cells.n
+    ctx = ilc.Context(0)
+    ctx.load_gaunt()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    d_rho, d_u, d_xe = (torch.from_numpy(a).to(dev) for a in (cells.rho, cells.u, cells.xe))
+    d_cells = torch.from_numpy(cells.xyzq(np.zeros(n, np.float32))).to(dev)
+    out = {"workload": "scale: 67,108,864 cells, 8 Mpc cube, two NFW halos 3:1 + 10 % "
+                       "background", "cells": n, "generate_s": t_gen}
+
+    def dev_time(fn):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    # per-cell flux + grid
+    for _ in range(2):
+        q, ms_q = dev_time(lambda: ctx.xray_flux(d_rho, d_u, d_xe, REDSHIFT, DL, E_MIN, E_MAX,
+                                                 NUM_SAMPLES))
+        xyzq = torch.cat([d_cells[:, :3], q[:, None]], dim=1).contiguous()
+        _, ms_g = dev_time(lambda: ctx.setup_particles(xyzq))
+    d = ctx.grid_describe()
+    gc, gs2u, gsrt = ctx.grid_export()
+    t0 = time.perf_counter()
+    og = oracle.Grid(xyzq.cpu().numpy())
+    oc, os2u, osrt, _ = og.export()
+    grid_ok = (np.array_equal(d["min_corner"], og.min_corner) and
+               np.array_equal(d["cell_sizes"], og.cell_sizes) and np.array_equal(gc, oc) and
+               np.array_equal(gs2u, os2u) and
+               np.array_equal(gsrt.view(np.uint32), osrt.view(np.uint32)))
+    t_og = time.perf_counter() - t0
+    del og, oc, os2u, osrt, gc, gs2u, gsrt
+    out["flux_ms"], out["grid_ms"] = ms_q, ms_g
+    out["grid"] = {"num_cells": [int(v) for v in d["num_cells"]],
+                   "bit_exact_vs_oracle": bool(grid_ok), "oracle_build_s": t_og}
+    # 2048^2 band map
+    cam = ilc.camera((box / 2, box / 2, 0.0), (0.0, 0.0, 1.0), 0.0, box, side, side)
+    d_img = torch.empty((side, side), dtype=torch.float32, device=dev)
+
+    def band_map():
+        return ctx.project_xray_flux(d_cells, d_rho, d_u, d_xe, cam, box, rel_tol=REL_TOL,
+                                     controller=ilc.CONTROLLER_FP64, e_min=E_MIN, e_max=E_MAX,
+                                     num_samples=NUM_SAMPLES, image=d_img)
+    band_map()  # warm-up (allocations, graph)
+    with ClockSampler(0) as clk:
+        (_, st), ms = dev_time(band_map)
+    out["band_map"] = {"image": [side, side], "z_range_kpc": box, "ms": ms,
+                       "kernel_ms": st["kernel_ms"], "mrays_per_s": side * side / ms * 1e3 / 1e6,
+                       "stats": st, "clocks": clk.summary()}
+    # adjoint, step checkpoints in row bands
+    img = d_img.cpu().numpy()
+    rng = np.random.default_rng(20174)
+    target = (img * np.exp(0.1 * rng.standard_normal(img.shape))).astype(np.float32)
+    ctx.set_checkpoint_budget(64 << 30)
+    xyz0 = cells.xyzq(np.zeros(n, np.float32))
+    with ClockSampler(0) as clk:
+        _, g_r, g_t, ast = ctx.adjoint_xray_flux(xyz0, cells.rho, cells.u, cells.xe, cam, box,
+                                                 target, mode=ilc._lib.ADJOINT_CHECKPOINT,
+                                                 rel_tol=REL_TOL, e_min=E_MIN, e_max=E_MAX,
+                                                 num_samples=NUM_SAMPLES)
+    cap = int(np.ceil(box / 0.2)) + 2
+    rows = min(side, max(8, (64 << 30) // (side * cap * 4) // 8 * 8))
+    out["adjoint"] = {"mode": "checkpoint", "checkpoint_budget_bytes": 64 << 30,
+                      "band_rows": rows, "bands": -(-side // rows),
+                      "forward_ms": ast["forward_ms"], "adjoint_ms": ast["adjoint_ms"],
+                      "quantity_ms": ast["quantity_ms"],
+                      "adjoint_over_forward": ast["adjoint_ms"] / ast["forward_ms"],
+                      "loss": ast["loss"], "finite": bool(np.all(np.isfinite(g_r)) and
+                                                          np.all(np.isfinite(g_t))),
+                      "clocks": clk.summary()}
+    del g_r, g_t
+    # 64-bin spectrum over a 512^2 aperture
+    edges = np.geomspace(0.3, 10.0, 65)
+    e = edges[:-1].astype(np.float32)
+    w = np.diff(edges).astype(np.float32)
+    tab, ms_t = dev_time(lambda: ctx.xray_spectrum(d_rho, d_u, d_xe, e, w))
+    ctx.setup_particles(xyzq)
+    scam = ilc.camera((box / 2, box / 2, 0.0), (0.0, 0.0, 1.0), 0.0, 4000.0, 512, 512)
+    job = [ilc.job(scam, z_range=box, aperture_radius=2000.0)]
+    ctx.render_batched(tab, job)  # warm-up: channel table sort, graph
+    (imgs, sst), ms_s = dev_time(lambda: ctx.render_batched(tab, job))
+    c = (np.arange(512) + 0.5 - 256) * (4000.0 / 512)
+    rays = int(np.sum(c[:, None] ** 2 + c[None, :] ** 2 <= 2000.0 ** 2))
+    out["spectrum"] = {"bins": 64, "image": [512, 512], "aperture_kpc": 2000.0, "rays": rays,
+                       "table_ms": ms_t, "ms": ms_s, "kernel_ms": sst["kernel_ms"],
+                       "mrays_per_s": rays / ms_s * 1e3 / 1e6,
+                       "mray_bins_per_s": rays * 64 / ms_s * 1e3 / 1e6, "stats": sst}
+    line = {"config": 4, "impl": "ours", "n_gpus": 1, "dtype": "f32",
+            "data": "synthetic (seeded, numpy PCG64 seed 20174)"}
+    line.update(out)
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -703,6 +831,9 @@ def main():
                     help="camera plane position along z (profiling cases only)")
     ap.add_argument("--z-range", type=float, default=None,
                     help="integration depth in kpc (default: the 6 Mpc box; profiling only)")
+    ap.add_argument("--config", type=int, default=1, choices=[1, 4],
+                    help="1: the band-map benchmark (default); 4: the 67 M-cell scale "
+                         "workload, one GPU, one pass of each of its parts")
     args = ap.parse_args()
     global NX, NY, Z_START, DEPTH
     NX = NY = args.image
@@ -716,6 +847,11 @@ def main():
         return
     from illcrawl_b200 import build
     build.build()
+    if args.config == 4:
+        if world > 1:
+            raise SystemExit("--config 4 runs on one GPU")
+        run_scale(args)
+        return
     if world > 1:
         import datetime
         import torch

@@ -26,6 +26,8 @@ import os
 import numpy as np
 
 from . import _lib
+QUERY_THREAD, QUERY_WARP = 0, 1
+
 from ._lib import (CONTROLLER_FP64, CONTROLLER_REF32, DA_INVERSE_RANGE, DA_PIXEL_AREA, DA_UNIT,
                    DV_MEAN, DV_VOLUME, ENGINE_GRID, ENGINE_PERSISTENT, Camera, IlcError, Job,
                    LosScaling, RenderStats, Tolerance)
@@ -506,6 +508,20 @@ class Context:
         return out[:k], idx[:k]
 
     # ---- batched render
+    def last_query_stats(self):
+        """(cells visited, candidates tested) of the last nn8_query."""
+        a, b = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        self.check(self.L.ilc_nn8_query_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
+
+    def set_query_engine(self, engine):
+        """QUERY_THREAD (0, default) or QUERY_WARP (1) for nn8 queries."""
+        self.check(self.L.ilc_set_query_engine(self.h, int(engine)))
+
+    def set_checkpoint_budget(self, nbytes):
+        """Device bytes the checkpoint adjoint may hold for step checkpoints."""
+        self.check(self.L.ilc_set_checkpoint_budget(self.h, int(nbytes)))
+
     def set_batch_schedule(self, tile_w=8, blocks_per_sm=4, z_window=40.0, cost_order=True):
         self.check(self.L.ilc_set_batch_schedule(self.h, int(tile_w), int(blocks_per_sm),
                                                  float(z_window), 1 if cost_order else 0))

@@ -115,6 +115,10 @@ SIGNATURES = {
     "ilc_render_record": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _P, _i64, _int, _P, _int, _P]),
     "ilc_render_frozen": (_int, [_P, _P, _f64, _P, _P, _i64, _int, _P, _P, _int, _P]),
     "ilc_render_ray_stats": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _P, _P, _int, _P]),
+    "ilc_set_checkpoint_budget": (_int, [_P, _u64]),
+    "ilc_set_query_engine": (_int, [_P, _i32]),
+    "ilc_nn8_query_stats": (_int, [_P, _P, _P]),
+    "ilc_render_frozen_f64": (_int, [_P, _P, _f64, _P, _P, _i64, _int, _P, _P, _int, _P]),
     "ilc_los_scale": (_f32, [_P, _f64, _P]),
     "ilc_project_xray_flux": (_int, [_P, _P, _P, _P, _P, _u64, _f32, _f32, _f32, _f32, _i32, _P,
                                      _f64, Tolerance, _i32, _P, _P, _int, _P]),

@@ -237,8 +237,9 @@ struct AdjK {
   const float* __restrict__ rec_h;  // checkpoint: accepted step sizes, ray-major
   const int32_t* __restrict__ rec_n;
   int64_t rec_cap;
-  const float* __restrict__ seed;  // dL/dI_raw per pixel
+  const float* __restrict__ seed;  // dL/dI_raw per pixel (whole image)
   double* __restrict__ grad;       // dL/dq per sorted particle
+  int row0, row_end;               // pixel rows of this launch; rec_* indexed from row0
 };
 
 __global__ void __launch_bounds__(128)
@@ -249,10 +250,10 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
   load_spiral(spiral, spiral_g);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int ix = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-  const int iy = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
-  if (ix >= a.cam.nx || iy >= a.cam.ny) return;
-  const int64_t ray = (int64_t)iy * a.cam.nx + ix;
-  const float gi = a.seed[ray];
+  const int iy = a.row0 + blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+  if (ix >= a.cam.nx || iy >= a.row_end) return;
+  const int64_t ray = (int64_t)(iy - a.row0) * a.cam.nx + ix;  // in the launch's rows
+  const float gi = a.seed[(int64_t)iy * a.cam.nx + ix];
   if (gi == 0.0f) return;
   float px, py, pz;
   pixel_corner(a.cam, ix, iy, px, py, pz);
@@ -349,9 +350,11 @@ cudaError_t adjoint_cell_launch(Context& c, const float* rho, const float* u, co
 }
 
 cudaError_t adjoint_seed_launch(Context& c, const float* img, const float* target, int64_t npix,
-                                float scale, float* seed, double* loss) {
-  cudaError_t e = cudaMemsetAsync(loss, 0, sizeof(double), c.stream);
-  if (e) return e;
+                                float scale, float* seed, double* loss, bool reset_loss) {
+  if (reset_loss) {
+    cudaError_t e = cudaMemsetAsync(loss, 0, sizeof(double), c.stream);
+    if (e) return e;
+  }
   ++c.launches;
   loss_seed_kernel<<<148 * 4, 256, 0, c.stream>>>(img, target, npix, scale, seed, loss);
   return cudaGetLastError();
@@ -379,8 +382,10 @@ cudaError_t adjoint_ray_launch(Context& c, const RenderArgs& r, int mode, const 
   k.rec_cap = r.rec_cap;
   k.seed = seed;
   k.grad = grad;
+  k.row0 = r.row0;
+  k.row_end = r.rows > 0 ? (r.row0 + r.rows < r.ny ? r.row0 + r.rows : r.ny) : r.ny;
   const GridView g = make_grid_view(c);
-  dim3 grid((r.nx + 15) / 16, (r.ny + 7) / 8);
+  dim3 grid((r.nx + 15) / 16, (k.row_end - k.row0 + 7) / 8);
   if (!c.ev0) {
     if ((e = cudaEventCreate(&c.ev0)) || (e = cudaEventCreate(&c.ev1))) return e;
   }

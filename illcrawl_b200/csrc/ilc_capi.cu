@@ -307,6 +307,7 @@ struct StepArrays {
   int32_t* rec_n = nullptr;
   int64_t cap = 0;
   uint64_t* ray_stats = nullptr;  // per-ray statistics (device)
+  double* out_d = nullptr;        // frozen replay summed in double (device image)
 };
 
 ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_tolerance tol,
@@ -315,7 +316,7 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
                          ilc_render_stats* stats, const StepArrays& sa = StepArrays()) {
   if (!c.has_grid) return fail(c, ILC_ERR_NO_PARTICLES, "render before setup_particles");
   if (!camera_ok(cam)) return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid camera");
-  if (!(z_range > 0.0) || !std::isfinite(z_range) || !image)
+  if (!(z_range > 0.0) || !std::isfinite(z_range) || (!image && !sa.out_d))
     return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid z_range or image");
   if (fixed_steps <= 0 && !sa.replay_h) {
     if (!(tol.absolute >= 0.0) || !(tol.relative >= 0.0) ||
@@ -344,9 +345,10 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
   a.rec_n = sa.rec_n;
   a.rec_cap = sa.cap;
   a.ray_stats = sa.ray_stats;
+  a.out_d = sa.out_d;
   const size_t bytes = (size_t)a.nx * (size_t)a.ny * 4;
   void* dimg = nullptr;
-  ILC_CUDA(c, out_ptr(c.out_a, image, bytes, is_device, &dimg), "image buffer");
+  if (image) ILC_CUDA(c, out_ptr(c.out_a, image, bytes, is_device, &dimg), "image buffer");
   a.out = static_cast<float*>(dimg);
   float ms = 0.0f;
   if (c.render_engine == ILC_ENGINE_PERSISTENT && fixed_steps <= 0 &&
@@ -364,7 +366,7 @@ ilc_status render_common(Context& c, const ilc_camera* cam, double z_range, ilc_
   } else {
     ILC_CUDA(c, render_launch(c, a, &ms), "render kernel");
   }
-  ILC_CUDA(c, finish_out(c, image, dimg, bytes, is_device), "render");
+  if (image) ILC_CUDA(c, finish_out(c, image, dimg, bytes, is_device), "render");
   uint32_t flags = 0;
   DevStats ds{};
   ilc_status st = read_flags(c, &flags, &ds);
@@ -920,10 +922,46 @@ ilc_status ilc_render_ray_stats(ilc_ctx* h, const ilc_camera* cam, double z_rang
   return st;
 }
 
+static ilc_status render_frozen_common(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                                       const float* step_sizes, const int32_t* n_steps,
+                                       int64_t capacity, int steps_on_device,
+                                       const ilc_los_scaling* scaling, float* image,
+                                       double* image_d, int is_device, ilc_render_stats* stats);
+
 ilc_status ilc_render_frozen(ilc_ctx* h, const ilc_camera* cam, double z_range,
                              const float* step_sizes, const int32_t* n_steps, int64_t capacity,
                              int steps_on_device, const ilc_los_scaling* scaling, float* image,
                              int is_device, ilc_render_stats* stats) {
+  if (!image) return ILC_ERR_INVALID_ARGUMENT;
+  return render_frozen_common(h, cam, z_range, step_sizes, n_steps, capacity, steps_on_device,
+                              scaling, image, nullptr, is_device, stats);
+}
+
+ilc_status ilc_render_frozen_f64(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                                 const float* step_sizes, const int32_t* n_steps,
+                                 int64_t capacity, int steps_on_device,
+                                 const ilc_los_scaling* scaling, double* image, int is_device,
+                                 ilc_render_stats* stats) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!image || !camera_ok(cam)) return fail(c, ILC_ERR_INVALID_ARGUMENT, "invalid image");
+  const uint64_t bytes = (uint64_t)cam->num_pix_x * (uint64_t)cam->num_pix_y * 8;
+  void* dimg = nullptr;
+  ILC_CUDA(c, out_ptr(c.out_c, image, bytes, is_device, &dimg), "double image buffer");
+  ilc_status st = render_frozen_common(h, cam, z_range, step_sizes, n_steps, capacity,
+                                       steps_on_device, scaling, nullptr,
+                                       static_cast<double*>(dimg), is_device, stats);
+  if (st) return st;
+  ILC_CUDA(c, finish_out(c, image, dimg, bytes, is_device), "double image D2H");
+  return ILC_OK;
+}
+
+static ilc_status render_frozen_common(ilc_ctx* h, const ilc_camera* cam, double z_range,
+                                       const float* step_sizes, const int32_t* n_steps,
+                                       int64_t capacity, int steps_on_device,
+                                       const ilc_los_scaling* scaling, float* image,
+                                       double* image_d, int is_device, ilc_render_stats* stats) {
   if (!h) return ILC_ERR_INVALID_ARGUMENT;
   Context& c = h->c;
   cudaSetDevice(c.device);
@@ -945,6 +983,7 @@ ilc_status ilc_render_frozen(ilc_ctx* h, const ilc_camera* cam, double z_range,
   sa.replay_h = static_cast<const float*>(dh);
   sa.replay_n = static_cast<const int32_t*>(dn);
   sa.cap = capacity;
+  sa.out_d = image_d;
   return render_common(c, cam, z_range, ilc_tolerance{0.0, 0.0}, ILC_CONTROLLER_REF32, 0,
                        scaling, image, is_device, stats, sa);
 }
@@ -987,6 +1026,34 @@ ilc_status ilc_project_xray_flux(ilc_ctx* h, const float* cells, const float* rh
 }
 
 uint64_t ilc_kernel_launches(const ilc_ctx* h) { return h ? h->c.launches : 0; }
+
+ilc_status ilc_nn8_query_stats(ilc_ctx* h, uint64_t* cells_visited, uint64_t* candidates) {
+  if (!h || !cells_visited || !candidates) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  if (!c.flags.p) return fail(c, ILC_ERR_INVALID_ARGUMENT, "no query has run on this context");
+  uint32_t flags = 0;
+  DevStats ds{};
+  ilc_status st = read_flags(c, &flags, &ds);
+  if (st) return st;
+  *cells_visited = ds.cells;
+  *candidates = ds.cands;
+  return ILC_OK;
+}
+
+ilc_status ilc_set_query_engine(ilc_ctx* h, int32_t engine) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  if (engine != ILC_QUERY_THREAD && engine != ILC_QUERY_WARP)
+    return fail(h->c, ILC_ERR_INVALID_ARGUMENT, "unknown query engine");
+  h->c.query_engine = engine;
+  return ILC_OK;
+}
+
+ilc_status ilc_set_checkpoint_budget(ilc_ctx* h, uint64_t bytes) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  h->c.checkpoint_budget = bytes;  // 0: a quarter of the device's memory
+  return ILC_OK;
+}
 
 ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rho,
                                  const float* u, const float* xe, uint64_t n, float redshift,
@@ -1037,7 +1104,12 @@ ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rh
   // 2. grid
   st = build_grid_staged(c, n);
   if (st) return st;
-  // 3. forward render, recording the accepted steps in CHECKPOINT mode
+  // 3-5. forward render (recording the accepted steps in CHECKPOINT mode),
+  // loss and per-pixel seed, adjoint rays: in bands of pixel rows whose step
+  // checkpoints (4 B x (ceil(z_range / 0.2 kpc) + 2) per ray, the most
+  // accepted steps a ray can take at the minimum step) fit the context's
+  // checkpoint budget. The seed of a pixel depends only on its own value, so
+  // each band runs forward -> seed -> adjoint before the next one starts.
   RenderArgs ra{};
   camera_plane(*cam, ra.cam);
   ra.nx = cam->num_pix_x;
@@ -1051,41 +1123,64 @@ ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rh
   ra.scale = scaling ? los_scale(*cam, z_range, *scaling) : 1.0f;
   ILC_CUDA(c, c.out_b.ensure((size_t)npix * 4), "image");
   ra.out = c.out_b.as<float>();
+  int32_t band_rows = ra.ny;
   if (mode == ILC_ADJOINT_CHECKPOINT) {
     ra.rec_cap = (int64_t)std::ceil(z_range / 0.2) + 2;
-    ILC_CUDA(c, c.rec_h.ensure((size_t)npix * (size_t)ra.rec_cap * 4),
+    const uint64_t per_row = (uint64_t)ra.nx * (uint64_t)ra.rec_cap * 4;
+    uint64_t budget = c.checkpoint_budget;
+    if (budget == 0) {
+      size_t free_b = 0, total_b = 0;
+      ILC_CUDA(c, cudaMemGetInfo(&free_b, &total_b), "device memory size");
+      budget = total_b / 4;
+    }
+    const uint64_t fit = budget / per_row;
+    band_rows = (int32_t)std::min<uint64_t>((uint64_t)ra.ny, std::max<uint64_t>(8, fit / 8 * 8));
+    ILC_CUDA(c, c.rec_h.ensure((size_t)band_rows * per_row),
              "step checkpoints (use ILC_ADJOINT_RECOMPUTE to avoid them)");
-    ILC_CUDA(c, c.rec_n.ensure((size_t)npix * 4), "step counts");
+    ILC_CUDA(c, c.rec_n.ensure((size_t)band_rows * ra.nx * 4), "step counts");
     ra.rec_h = c.rec_h.as<float>();
     ra.rec_n = c.rec_n.as<int32_t>();
   }
-  float fwd_ms = 0.0f;
-  ILC_CUDA(c, render_launch(c, ra, &fwd_ms), "forward render");
-  uint32_t flags = 0;
-  DevStats fs{};
-  st = read_flags(c, &flags, &fs);
-  if (st) return st;
-  if (flags & FLAG_STEP_LIMIT) return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the step limit");
-  if (flags & FLAG_REC_OVERFLOW) return fail(c, ILC_ERR_INTERNAL, "step checkpoint overflow");
-  // 4. loss and per-pixel seed
   const void* dtarget = nullptr;
   ILC_CUDA(c, stage_in(c, c.in_a, target, (size_t)npix * 4, is_device, &dtarget), "target");
   ILC_CUDA(c, c.adj_seed.ensure((size_t)npix * 4), "seed");
   ILC_CUDA(c, c.adj_loss.ensure(8), "loss");
-  ILC_CUDA(c, adjoint_seed_launch(c, ra.out, static_cast<const float*>(dtarget), npix, ra.scale,
-                                  c.adj_seed.as<float>(), c.adj_loss.as<double>()),
-           "loss kernel");
-  // 5. adjoint rays
+  ILC_CUDA(c, cudaMemsetAsync(c.adj_loss.p, 0, 8, c.stream), "loss");
   ILC_CUDA(c, c.adj_grad.ensure(n * 8), "gradient");
   ILC_CUDA(c, cudaMemsetAsync(c.adj_grad.p, 0, n * 8, c.stream), "gradient");
-  float adj_ms = 0.0f;
-  ILC_CUDA(c, adjoint_ray_launch(c, ra, mode, c.adj_seed.as<float>(), c.adj_grad.as<double>(),
-                                 &adj_ms),
-           "adjoint kernel");
-  DevStats as{};
-  st = read_flags(c, &flags, &as);
-  if (st) return st;
-  if (flags & FLAG_STEP_LIMIT) return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the step limit");
+  float fwd_ms = 0.0f, adj_ms = 0.0f;
+  uint64_t fwd_steps = 0, adj_steps = 0;
+  uint32_t flags = 0;
+  for (int32_t row0 = 0; row0 < ra.ny; row0 += band_rows) {
+    ra.row0 = row0;
+    ra.rows = std::min(band_rows, ra.ny - row0);
+    float ms = 0.0f;
+    ILC_CUDA(c, render_launch(c, ra, &ms), "forward render");
+    fwd_ms += ms;
+    DevStats fs{};
+    st = read_flags(c, &flags, &fs);
+    if (st) return st;
+    if (flags & FLAG_STEP_LIMIT)
+      return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the step limit");
+    if (flags & FLAG_REC_OVERFLOW) return fail(c, ILC_ERR_INTERNAL, "step checkpoint overflow");
+    fwd_steps += fs.steps;
+    const size_t off = (size_t)row0 * ra.nx;
+    ILC_CUDA(c, adjoint_seed_launch(c, ra.out + off, static_cast<const float*>(dtarget) + off,
+                                    (int64_t)ra.rows * ra.nx, ra.scale,
+                                    c.adj_seed.as<float>() + off, c.adj_loss.as<double>(),
+                                    false),
+             "loss kernel");
+    ILC_CUDA(c, adjoint_ray_launch(c, ra, mode, c.adj_seed.as<float>(), c.adj_grad.as<double>(),
+                                   &ms),
+             "adjoint kernel");
+    adj_ms += ms;
+    DevStats as{};
+    st = read_flags(c, &flags, &as);
+    if (st) return st;
+    if (flags & FLAG_STEP_LIMIT)
+      return fail(c, ILC_ERR_STEP_LIMIT, "rays reached the step limit");
+    adj_steps += as.steps;
+  }
   // 6. chain rule into the caller's arrays
   void *gr = nullptr, *gt = nullptr;
   ILC_CUDA(c, out_ptr(c.out_a, dL_dlnrho, n * 4, is_device, &gr), "dL/dlnrho");
@@ -1112,8 +1207,8 @@ ilc_status ilc_adjoint_xray_flux(ilc_ctx* h, const float* cells, const float* rh
     stats->quantity_ms = qms;
     stats->forward_ms = fwd_ms;
     stats->adjoint_ms = adj_ms;
-    stats->forward_steps = fs.steps;
-    stats->adjoint_steps = as.steps;
+    stats->forward_steps = fwd_steps;
+    stats->adjoint_steps = adj_steps;
   }
   return ILC_OK;
 }

@@ -51,9 +51,12 @@ struct Context {
   bool own_stream = false;
   std::string error;
   int64_t max_steps = 1 << 20;  // per-ray RKF step cap
+  uint64_t checkpoint_budget = 0;  // adjoint: device bytes for step checkpoints (0: a quarter
+                                   // of the device's memory)
   float z_window = 0.0f;        // adaptive render: z window of the block schedule (0 = none)
   int32_t render_occupancy = 4; // adaptive render: blocks per SM (0 = register-limited)
   int32_t render_engine = ILC_ENGINE_PERSISTENT;  // FP64 adaptive renders: kernel used
+  int32_t query_engine = ILC_QUERY_THREAD;        // ilc_nn8_query: one thread or one warp per query
 
   // particle grid
   bool has_grid = false;
@@ -194,6 +197,7 @@ struct RenderArgs {
   float scale;          // multiplier applied to each pixel
   bool apply_scale;
   float* out;           // device image
+  double* out_d = nullptr;  // frozen replay: device image of the increments summed in double
   float window_override = -1.0f;  // >= 0: z window for this launch (autotuner)
   int occupancy_override = -1;    // >= 0: occupancy variant for this launch (autotuner)
   int row_stride = 1;             // > 1: only every row_stride-th tile row (autotuner)
@@ -203,6 +207,9 @@ struct RenderArgs {
   const float* replay_h = nullptr;    // frozen replay: per-ray step sizes (rec_cap each)
   const int32_t* replay_n = nullptr;  // frozen replay: steps per ray
   uint64_t* ray_stats = nullptr;      // optional: per ray (steps, accepted, cells, candidates)
+  int32_t row0 = 0;   // first pixel row of this launch (a multiple of 8)
+  int32_t rows = 0;   // pixel rows of this launch (0: to the last row); per-ray arrays
+                      // (rec_h, rec_n, replay_*, ray_stats) are indexed from row0
 };
 
 // Adjoint of the X-ray band map (ilc_adjoint.cu).
@@ -213,8 +220,9 @@ cudaError_t adjoint_cell_launch(Context& c, const float* rho, const float* u, co
                                 float* dq_lnrho);
 // loss (double, accumulated) and dL/dI_raw seed per pixel
 cudaError_t adjoint_seed_launch(Context& c, const float* img, const float* target, int64_t npix,
-                                float scale, float* seed, double* loss);
-// replay (checkpoint) or recompute the rays and scatter dL/dq (sorted order)
+                                float scale, float* seed, double* loss, bool reset_loss = true);
+// replay (checkpoint) or recompute the rays of the band [a.row0, a.row0 + a.rows)
+// and scatter dL/dq (sorted order); seed is indexed by the full image's pixels
 cudaError_t adjoint_ray_launch(Context& c, const RenderArgs& a, int mode, const float* seed,
                                double* grad, float* kernel_ms);
 // dL/dln rho, dL/dln T in the original order

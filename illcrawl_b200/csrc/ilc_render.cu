@@ -7,6 +7,7 @@
 // nn8 walk inline. A ray's state depends only on its own evaluations, so this
 // is the same computation as the reference's lock-step loop with stream
 // compaction, without its per-iteration host synchronisations.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -49,12 +50,15 @@ struct RenderK {
   int64_t max_steps;
   float window;     // z window of the adaptive schedule (<= 0: none)
   int row_stride;   // render every row_stride-th row of tiles (1 = all)
+  int row0;         // first pixel row (a multiple of the tile height)
+  int row_end;      // one past the last pixel row
   float* rec_h;     // optional: accepted step sizes per ray (ray-major, rec_cap each)
   int32_t* rec_n;   // optional: number of accepted steps per ray
   int64_t rec_cap;
   float scale;
   int apply_scale;
   float* out;
+  double* out_d;        // optional (frozen replay): the line integrals summed in double
   uint64_t* ray_stats;  // optional: per ray (steps, accepted, cells visited, candidates)
 };
 
@@ -62,10 +66,10 @@ struct RenderK {
 // 8 x 4 tile, so the 32 rays of a warp are spatial neighbours.
 constexpr int kRenderThreads = 128;
 constexpr int kTileX = 16, kTileY = 8;
-__device__ __forceinline__ void block_pixel(int row_stride, int& ix, int& iy) {
+__device__ __forceinline__ void block_pixel(int row_stride, int row0, int& ix, int& iy) {
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   ix = blockIdx.x * kTileX + (warp & 1) * 8 + (lane & 7);
-  iy = blockIdx.y * row_stride * kTileY + (warp >> 1) * 4 + (lane >> 3);
+  iy = row0 + blockIdx.y * row_stride * kTileY + (warp >> 1) * 4 + (lane >> 3);
 }
 
 template <int kMinBlocks>
@@ -76,8 +80,10 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
   __shared__ SlotMem slot_mem;
   load_spiral(spiral, spiral_g);
   int ix, iy;
-  block_pixel(a.row_stride, ix, iy);
-  const bool active = ix < a.cam.nx && iy < a.cam.ny;
+  block_pixel(a.row_stride, a.row0, ix, iy);
+  const bool active = ix < a.cam.nx && iy < a.row_end;
+  // per-ray arrays are indexed from the launch's first row
+  const int64_t lray = (int64_t)(iy - a.row0) * a.cam.nx + ix;
   WalkStats ws;
   unsigned long long steps = 0, acc = 0;
   bool at_limit = false;
@@ -85,14 +91,14 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
   if (active) pixel_corner(a.cam, ix, iy, px, py, pz);
   const float lx = a.cam.look0, ly = a.cam.look1, lz = a.cam.look2;
   float I = 0.0f, z = a.z0, h = 1.0f, k1 = 0.0f;
+  double Id = 0.0;  // out_d: the same increments summed in double
   float pts[4];
   if (a.replay_h) {
     if (active) {
       // Frozen per-ray sequence: the given steps, every one accepted.
-      const int64_t ray = (int64_t)iy * a.cam.nx + ix;
-      const int64_t nr = a.replay_n[ray];
+      const int64_t nr = a.replay_n[lray];
       const int32_t n = (int32_t)(nr < 0 ? 0 : (nr > a.rec_cap ? a.rec_cap : nr));
-      const float* hs = a.replay_h + ray * a.rec_cap;
+      const float* hs = a.replay_h + lray * a.rec_cap;
       for (int32_t s = 0; s < n; ++s) {
         h = hs[s];
         rkf_points(z, h, pts);
@@ -102,6 +108,7 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
                    1.f / 5.f * e[2];
         d4 *= h;
         I = I + d4;
+        if (a.out_d) Id += (double)d4;
         z += h;
         k1 = e[2];
       }
@@ -146,20 +153,22 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
         ++steps;
         if (z != zb) {
           if (a.rec_h && (int64_t)acc < a.rec_cap)
-            a.rec_h[((int64_t)iy * a.cam.nx + ix) * a.rec_cap + (int64_t)acc] = hb;
+            a.rec_h[lray * a.rec_cap + (int64_t)acc] = hb;
           ++acc;
         }
       }
       wend = a.window > 0.0f ? wend + a.window : a.z_end;
     }
     if (active && a.rec_n) {
-      a.rec_n[(int64_t)iy * a.cam.nx + ix] = (int32_t)min((int64_t)acc, a.rec_cap);
+      a.rec_n[lray] = (int32_t)min((int64_t)acc, a.rec_cap);
       if ((int64_t)acc > a.rec_cap) atomicOr(flags, FLAG_REC_OVERFLOW);
     }
   }
-  if (active) a.out[(size_t)iy * a.cam.nx + ix] = a.apply_scale ? I * a.scale : I;
+  if (active && a.out) a.out[(size_t)iy * a.cam.nx + ix] = a.apply_scale ? I * a.scale : I;
+  if (active && a.out_d)
+    a.out_d[(size_t)iy * a.cam.nx + ix] = a.apply_scale ? Id * (double)a.scale : Id;
   if (active && a.ray_stats) {
-    uint64_t* r = a.ray_stats + 4 * ((size_t)iy * a.cam.nx + ix);
+    uint64_t* r = a.ray_stats + 4 * lray;
     r[0] = steps;
     r[1] = acc;
     r[2] = ws.cells;
@@ -212,15 +221,18 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   k.max_steps = c.max_steps;
   k.window = a.window_override >= 0.0f ? a.window_override : c.z_window;
   k.row_stride = a.row_stride > 1 ? a.row_stride : 1;
+  k.row0 = a.row0;
+  k.row_end = a.rows > 0 ? std::min(a.ny, a.row0 + a.rows) : a.ny;
   k.rec_h = a.rec_h;
   k.rec_n = a.rec_n;
   k.rec_cap = a.rec_cap;
   k.scale = a.scale;
   k.apply_scale = a.apply_scale ? 1 : 0;
   k.out = a.out;
+  k.out_d = a.out_d;
   k.ray_stats = a.ray_stats;
   const GridView g = make_grid_view(c);
-  const int tile_rows = (a.ny + kTileY - 1) / kTileY;
+  const int tile_rows = (k.row_end - k.row0 + kTileY - 1) / kTileY;
   dim3 grid((a.nx + kTileX - 1) / kTileX, (tile_rows + k.row_stride - 1) / k.row_stride);
   if (!c.ev0) {
     if ((e = cudaEventCreate(&c.ev0)) || (e = cudaEventCreate(&c.ev1))) return e;

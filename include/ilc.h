@@ -120,6 +120,21 @@ ilc_status ilc_set_z_window(ilc_ctx* ctx, float z_window);
 enum { ILC_ENGINE_GRID = 0, ILC_ENGINE_PERSISTENT = 1 };
 ilc_status ilc_set_render_engine(ilc_ctx* ctx, int32_t engine);
 
+/* Kernel of ilc_nn8_query (and of the consumers that query through it):
+ * ILC_QUERY_THREAD (default) walks each query in one thread, as the
+ * reference's kernel does; ILC_QUERY_WARP walks each query with a whole warp
+ * (the cells of the spiral and the candidates tested 32 at a time, hits
+ * collected by ballot and inserted in candidate order). Both give the same
+ * results bit for bit. No reference counterpart. */
+enum { ILC_QUERY_THREAD = 0, ILC_QUERY_WARP = 1 };
+ilc_status ilc_set_query_engine(ilc_ctx* ctx, int32_t engine);
+
+/* Search counters of the last ilc_nn8_query on this context: grid cells
+ * visited and candidate particles tested, summed over its queries (the
+ * oracle's counters; the traffic model of the walk). Valid until the next
+ * call that launches a kernel. No reference counterpart. */
+ilc_status ilc_nn8_query_stats(ilc_ctx* ctx, uint64_t* cells_visited, uint64_t* candidates);
+
 /* Occupancy of the adaptive render: 0 = as many blocks per SM as the
  * kernel's registers allow, 3, 4 or 5 = that many 128-thread blocks per SM
  * (registers capped accordingly). Changes the order of work only, never a
@@ -301,6 +316,18 @@ ilc_status ilc_render_frozen(ilc_ctx* ctx, const ilc_camera* cam, double z_range
                              const float* step_sizes, const int32_t* n_steps, int64_t capacity,
                              int steps_on_device, const ilc_los_scaling* scaling, float* image,
                              int is_device, ilc_render_stats* stats);
+
+/* ilc_render_frozen with each ray's fp32 step increments summed in double
+ * into a double image (num_pix_y x num_pix_x, follows is_device). The fp32
+ * walk and increments are the frozen replay's, so two replays that differ
+ * only in a few particles' values differ only in the increments those values
+ * enter: finite-difference checks of the adjoint read the difference without
+ * the fp32 accumulation's rounding. No reference counterpart. */
+ilc_status ilc_render_frozen_f64(ilc_ctx* ctx, const ilc_camera* cam, double z_range,
+                                 const float* step_sizes, const int32_t* n_steps,
+                                 int64_t capacity, int steps_on_device,
+                                 const ilc_los_scaling* scaling, double* image, int is_device,
+                                 ilc_render_stats* stats);
 
 /* The multiplier applied to every pixel by volumetric_integration.cpp:74-87. */
 float ilc_los_scale(const ilc_camera* cam, double z_range, const ilc_los_scaling* scaling);
@@ -498,7 +525,11 @@ ilc_status ilc_autotune_batched(ilc_ctx* ctx, const float* values, int32_t n_cha
  * from the forward pass. No reference counterpart (the reference has no
  * differentiation). CHECKPOINT stores every ray's accepted step sizes during
  * the forward pass (4 B x (z_range / 0.2 + 2) per ray of device memory) and
- * replays them; RECOMPUTE runs the step controller again instead. Pixels whose
+ * replays them; the image is processed in bands of pixel rows (multiples of
+ * 8) whose checkpoints fit the context's budget (ilc_set_checkpoint_budget,
+ * default a quarter of the device's memory), each band forward, seeded and
+ * replayed before the next, so
+ * any image size fits. RECOMPUTE runs the step controller again instead. Pixels whose
  * value or target is not positive are left out of L. The per-cell factors
  * dq/dln rho and dq/dln T are exact derivatives of the adaptive energy
  * integration of xray_flux. image receives the forward band map. */
@@ -512,6 +543,11 @@ typedef struct ilc_adjoint_stats {
   uint64_t forward_steps;
   uint64_t adjoint_steps;
 } ilc_adjoint_stats;
+
+/* Device memory the CHECKPOINT adjoint may use for step checkpoints (bytes;
+ * 0 = a quarter of the device's memory, the default; at least one band of 8
+ * pixel rows is always used). No reference counterpart. */
+ilc_status ilc_set_checkpoint_budget(ilc_ctx* ctx, uint64_t bytes);
 
 ilc_status ilc_adjoint_xray_flux(ilc_ctx* ctx, const float* cells, const float* rho,
                                  const float* u, const float* xe, uint64_t n, float redshift,

@@ -75,3 +75,28 @@ def test_gpu_adjoint_checkpoint_equals_recompute(ctx, oracle_mod, gaunt_table):
     assert np.linalg.norm(r0 - r1) / np.linalg.norm(r0) < 1e-5
     assert np.linalg.norm(t0 - t1) / np.linalg.norm(t0) < 1e-5
     assert s0["loss"] == pytest.approx(s1["loss"], rel=1e-12)
+
+
+def test_gpu_adjoint_checkpoint_in_row_bands(ctx, oracle_mod, gaunt_table):
+    """A checkpoint budget of one 8-row band: the image is processed in 3
+    bands (forward, seed, replay each); image and loss equal the one-band
+    run, the gradient up to the atomics' summation order."""
+    ilc, c, args, q, dqT, dqR, g, I, hs, nacc, target = _setup(oracle_mod, gaunt_table, seed=43)
+    ctx.load_gaunt()
+    cells = c.xyzq(np.zeros(c.n, np.float32))
+    t = target.reshape(args[5], args[4])
+    i0, r0, t0, s0 = ctx.adjoint_xray_flux(cells, c.rho, c.u, c.xe, ilc.camera(*args), 400.0, t,
+                                           mode=0)
+    cap = int(np.ceil(400.0 / 0.2)) + 2
+    ctx.set_checkpoint_budget(8 * args[4] * cap * 4)
+    try:
+        i1, r1, t1, s1 = ctx.adjoint_xray_flux(cells, c.rho, c.u, c.xe, ilc.camera(*args), 400.0,
+                                               t, mode=0)
+    finally:
+        ctx.set_checkpoint_budget(0)
+    assert np.array_equal(i0.view(np.uint32), i1.view(np.uint32))
+    assert s0["forward_steps"] == s1["forward_steps"]
+    assert s0["adjoint_steps"] == s1["adjoint_steps"]
+    assert s0["loss"] == pytest.approx(s1["loss"], rel=1e-12)
+    assert np.linalg.norm(r0 - r1) / np.linalg.norm(r0) < 1e-5
+    assert np.linalg.norm(t0 - t1) / np.linalg.norm(t0) < 1e-5
