@@ -240,17 +240,19 @@ struct AdjK {
   const float* __restrict__ seed;  // dL/dI_raw per pixel (whole image)
   double* __restrict__ grad;       // dL/dq per sorted particle
   int row0, row_end;               // pixel rows of this launch; rec_* indexed from row0
+  unsigned* queue;                 // persistent launch: tile counter (nullptr: block per tile)
+  unsigned ntiles, tiles_x;
 };
 
-__global__ void __launch_bounds__(128)
-adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
-               uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
-  __shared__ char4 spiral[1000];
-  __shared__ SlotMem slot_mem;
-  load_spiral(spiral, spiral_g);
+// The rays of one 16 x 8 tile (one per thread; no block synchronisation).
+__device__ __forceinline__ void adjoint_tile(const AdjK& a, const GridView& g,
+                                             const char4* __restrict__ spiral, SlotMem& slot_mem,
+                                             uint32_t* __restrict__ flags,
+                                             unsigned long long* __restrict__ stats, int bx,
+                                             int by) {
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int ix = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-  const int iy = a.row0 + blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+  const int ix = bx * 16 + (warp & 1) * 8 + (lane & 7);
+  const int iy = a.row0 + by * 8 + (warp >> 1) * 4 + (lane >> 3);
   if (ix >= a.cam.nx || iy >= a.row_end) return;
   const int64_t ray = (int64_t)(iy - a.row0) * a.cam.nx + ix;  // in the launch's rows
   const float gi = a.seed[(int64_t)iy * a.cam.nx + ix];
@@ -315,6 +317,30 @@ adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
   atomicAdd(&stats[0], steps);
   atomicAdd(&stats[3], c);
   atomicAdd(&stats[4], k);
+}
+
+// Persistent: the resident blocks take tiles from a queue (one block per tile
+// without one), as the render kernel does.
+__global__ void __launch_bounds__(128)
+adjoint_kernel(AdjK a, GridView g, const char4* __restrict__ spiral_g,
+               uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
+  __shared__ char4 spiral[1000];
+  __shared__ SlotMem slot_mem;
+  __shared__ unsigned next_tile;
+  load_spiral(spiral, spiral_g);
+  if (!a.queue) {
+    adjoint_tile(a, g, spiral, slot_mem, flags, stats, blockIdx.x, blockIdx.y);
+    return;
+  }
+  for (;;) {
+    if (threadIdx.x == 0) next_tile = atomicAdd(a.queue, 1u);
+    __syncthreads();
+    const unsigned t = next_tile;
+    __syncthreads();
+    if (t >= a.ntiles) break;
+    adjoint_tile(a, g, spiral, slot_mem, flags, stats, (int)(t % a.tiles_x),
+                 (int)(t / a.tiles_x));
+  }
 }
 
 // dL/dln rho and dL/dln T in the original particle order.
@@ -386,6 +412,22 @@ cudaError_t adjoint_ray_launch(Context& c, const RenderArgs& r, int mode, const 
   k.row_end = r.rows > 0 ? (r.row0 + r.rows < r.ny ? r.row0 + r.rows : r.ny) : r.ny;
   const GridView g = make_grid_view(c);
   dim3 grid((r.nx + 15) / 16, (k.row_end - k.row0 + 7) / 8);
+  k.queue = nullptr;
+  k.tiles_x = grid.x;
+  k.ntiles = grid.x * grid.y;
+  {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    const cudaError_t oe =
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 128, 0);
+    const unsigned resident = (unsigned)((sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1));
+    if (oe == cudaSuccess && k.ntiles > resident) {
+      if ((e = c.tile_queue.ensure(256))) return e;
+      if ((e = cudaMemsetAsync(c.tile_queue.p, 0, 4, c.stream))) return e;
+      k.queue = c.tile_queue.as<unsigned>();
+      grid = dim3(resident, 1);
+    }
+  }
   if (!c.ev0) {
     if ((e = cudaEventCreate(&c.ev0)) || (e = cudaEventCreate(&c.ev1))) return e;
   }

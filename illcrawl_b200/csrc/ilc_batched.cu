@@ -49,6 +49,7 @@ struct BatchK {
   float window;
   const uint32_t* order;
   unsigned long long* queue;
+  int axis_z;       // every job looks along z (look x and y exactly 0)
 };
 
 // Largest k with jobs[k].item_begin <= item.
@@ -167,7 +168,7 @@ __device__ __forceinline__ float channel_step(float Ic, float k1c, float e0, flo
 // kMulti: V > 1 channels from the table. kOwnVal (V = 1 without a channel
 // table): the slots carry the particles' own q, as the render kernel's walk
 // does, so no value is looked up by index afterwards.
-template <bool kMulti, int kMinBlocks, bool kOwnVal>
+template <bool kMulti, int kMinBlocks, bool kOwnVal, bool kAxis = false>
 __global__ void __launch_bounds__(kBThreads, kMinBlocks)
 batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
                uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
@@ -235,7 +236,7 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
       if (go) {
         Step4 s;
         s4_bind(s, slot_mem);
-        nn8_walk_step4<!kOwnVal>(g, spiral, o[0], o[1], o[2], lx, ly, lz, pts, s, ws);
+        nn8_walk_step4<!kOwnVal, kAxis>(g, spiral, o[0], o[1], o[2], lx, ly, lz, pts, s, ws);
         if (!kMulti) {
           float e[4];
           if (kOwnVal) {
@@ -476,8 +477,12 @@ cudaError_t launch_variant(Context& c, const BatchK& k, const GridView& g, int b
   unsigned long long* stats = reinterpret_cast<unsigned long long*>(c.flags.as<char>() + 64);
   if constexpr (!kMulti) {
     if (!k.chan) {
-      batched_kernel<false, kMinBlocks, true><<<blocks, kBThreads, 0, c.stream>>>(
-          k, g, c.spiral.as<char4>(), c.flags.as<uint32_t>(), stats);
+      if (k.axis_z)
+        batched_kernel<false, kMinBlocks, true, true><<<blocks, kBThreads, 0, c.stream>>>(
+            k, g, c.spiral.as<char4>(), c.flags.as<uint32_t>(), stats);
+      else
+        batched_kernel<false, kMinBlocks, true><<<blocks, kBThreads, 0, c.stream>>>(
+            k, g, c.spiral.as<char4>(), c.flags.as<uint32_t>(), stats);
       return cudaGetLastError();
     }
   }
@@ -578,6 +583,7 @@ cudaError_t batched_launch(Context& c, const BatchArgs& a, float* kernel_ms) {
   k.window = a.window;
   k.order = a.order;
   k.queue = c.queue.as<unsigned long long>();
+  k.axis_z = a.axis_z ? 1 : 0;
   const int occ = a.occupancy;
   const int blocks = variant_blocks(c, a.V > 1, occ);
   if (a.V > 1) {

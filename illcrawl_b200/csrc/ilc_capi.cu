@@ -272,6 +272,9 @@ ilc_status batched_jobs(Context& c, int32_t V, const ilc_job* jobs, int32_t n_jo
   a->occupancy = c.batch_occupancy;
   a->window = c.batch_window;
   a->order = nullptr;
+  a->axis_z = true;
+  for (const JobDev& d : jd)
+    if (d.look[0] != 0.0f || d.look[1] != 0.0f) a->axis_z = false;
   if (c.batch_cost_order) ILC_CUDA(c, batched_order(c, *a, jd), "work order");
   return ILC_OK;
 }

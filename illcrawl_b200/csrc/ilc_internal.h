@@ -87,6 +87,7 @@ struct Context {
 
   // generic per-call staging
   DevBuf in_a, in_b, in_c, out_a, out_b, out_c;
+  DevBuf tile_queue;  // persistent one-block-per-tile kernels: tile counter
   DevBuf spiral;     // char4[1000]
   DevBuf flags;      // uint32 error flags + uint64 stats
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -256,6 +257,7 @@ struct BatchArgs {
   int32_t occupancy;      // 0, 3 or 4
   float window;           // per-warp z window (0 = none)
   const uint32_t* order;  // device: work item handed out q-th (nullptr = natural order)
+  bool axis_z = false;    // every job looks along z (look x and y exactly 0)
 };
 // Estimated cost per work item of a batched render (the particles projected
 // into each tile's pixel columns, weighted by their cell's occupancy), and

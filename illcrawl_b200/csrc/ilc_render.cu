@@ -32,7 +32,14 @@ GridView make_grid_view(const Context& c) {
   g.inv_w0 = 4.0f / c.gp.cs[0];
   g.inv_w1 = 4.0f / c.gp.cs[1];
   g.inv_w2 = 4.0f / c.gp.cs[2];
-  g.margin = std::fmax(std::fmax(c.gp.cs[0], c.gp.cs[1]), c.gp.cs[2]) / 1024.0f;
+  // slack for the float rounding of cell keys and cell boxes: a 1024th of a
+  // cell, and at least 8 ulp of the largest coordinate of the grid
+  float ext = 0.0f;
+  for (int k = 0; k < 3; ++k)
+    ext = std::fmax(ext, std::fmax(std::fabs(c.gp.min[k]),
+                                   std::fabs(c.gp.min[k] + (float)c.gp.n[k] * c.gp.cs[k])));
+  g.margin = std::fmax(std::fmax(std::fmax(c.gp.cs[0], c.gp.cs[1]), c.gp.cs[2]) / 1024.0f,
+                       ext * 9.5367431640625e-07f);
   return g;
 }
 
@@ -60,27 +67,30 @@ struct RenderK {
   float* out;
   double* out_d;        // optional (frozen replay): the line integrals summed in double
   uint64_t* ray_stats;  // optional: per ray (steps, accepted, cells visited, candidates)
+  unsigned* queue;      // persistent launch: tile counter (nullptr: one block per tile)
+  unsigned ntiles, tiles_x;
 };
 
 // Pixel tiling: a block of 128 threads covers 16 x 8 pixels; each warp an
 // 8 x 4 tile, so the 32 rays of a warp are spatial neighbours.
 constexpr int kRenderThreads = 128;
 constexpr int kTileX = 16, kTileY = 8;
-__device__ __forceinline__ void block_pixel(int row_stride, int row0, int& ix, int& iy) {
+__device__ __forceinline__ void block_pixel(int row_stride, int row0, int bx, int by, int& ix,
+                                            int& iy) {
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  ix = blockIdx.x * kTileX + (warp & 1) * 8 + (lane & 7);
-  iy = row0 + blockIdx.y * row_stride * kTileY + (warp >> 1) * 4 + (lane >> 3);
+  ix = bx * kTileX + (warp & 1) * 8 + (lane & 7);
+  iy = row0 + by * row_stride * kTileY + (warp >> 1) * 4 + (lane >> 3);
 }
 
-template <int kMinBlocks>
-__global__ void __launch_bounds__(kRenderThreads, kMinBlocks)
-render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
-              uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
-  __shared__ char4 spiral[1000];
-  __shared__ SlotMem slot_mem;
-  load_spiral(spiral, spiral_g);
+// One 16 x 8 tile of rays, all threads of the block (the adaptive branch
+// synchronises the block at every z window).
+__device__ __forceinline__ void render_tile(const RenderK& a, const GridView& g,
+                                            const char4* __restrict__ spiral, SlotMem& slot_mem,
+                                            uint32_t* __restrict__ flags,
+                                            unsigned long long* __restrict__ stats, int bx,
+                                            int by) {
   int ix, iy;
-  block_pixel(a.row_stride, a.row0, ix, iy);
+  block_pixel(a.row_stride, a.row0, bx, by, ix, iy);
   const bool active = ix < a.cam.nx && iy < a.row_end;
   // per-ray arrays are indexed from the launch's first row
   const int64_t lray = (int64_t)(iy - a.row0) * a.cam.nx + ix;
@@ -198,6 +208,33 @@ render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
   }
 }
 
+// Persistent: the resident blocks take tiles (row-major) from a queue until
+// none is left, so the blocks that finish early take on more tiles instead of
+// idling while the slowest tiles of a wave finish. Without a queue, one block
+// per tile.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kRenderThreads, kMinBlocks)
+render_kernel(RenderK a, GridView g, const char4* __restrict__ spiral_g,
+              uint32_t* __restrict__ flags, unsigned long long* __restrict__ stats) {
+  __shared__ char4 spiral[1000];
+  __shared__ SlotMem slot_mem;
+  __shared__ unsigned next_tile;
+  load_spiral(spiral, spiral_g);
+  if (!a.queue) {
+    render_tile(a, g, spiral, slot_mem, flags, stats, blockIdx.x, blockIdx.y);
+    return;
+  }
+  for (;;) {
+    if (threadIdx.x == 0) next_tile = atomicAdd(a.queue, 1u);
+    __syncthreads();
+    const unsigned t = next_tile;
+    __syncthreads();
+    if (t >= a.ntiles) break;
+    render_tile(a, g, spiral, slot_mem, flags, stats, (int)(t % a.tiles_x),
+                (int)(t / a.tiles_x));
+  }
+}
+
 }  // namespace
 
 cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
@@ -234,12 +271,36 @@ cudaError_t render_launch(Context& c, const RenderArgs& a, float* kernel_ms) {
   const GridView g = make_grid_view(c);
   const int tile_rows = (k.row_end - k.row0 + kTileY - 1) / kTileY;
   dim3 grid((a.nx + kTileX - 1) / kTileX, (tile_rows + k.row_stride - 1) / k.row_stride);
+  const int occ = a.occupancy_override >= 0 ? a.occupancy_override : c.render_occupancy;
+  k.queue = nullptr;
+  k.tiles_x = grid.x;
+  k.ntiles = grid.x * grid.y;
+  {
+    // persistent blocks, as many as are resident
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    cudaError_t oe =
+        occ == 5   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<5>,
+                                                                   kRenderThreads, 0)
+        : occ == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<4>,
+                                                                   kRenderThreads, 0)
+        : occ == 3 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<3>,
+                                                                   kRenderThreads, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<1>,
+                                                                   kRenderThreads, 0);
+    const unsigned resident = (unsigned)((sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1));
+    if (oe == cudaSuccess && k.ntiles > resident) {
+      if ((e = c.tile_queue.ensure(256))) return e;
+      if ((e = cudaMemsetAsync(c.tile_queue.p, 0, 4, c.stream))) return e;
+      k.queue = c.tile_queue.as<unsigned>();
+      grid = dim3(resident, 1);
+    }
+  }
   if (!c.ev0) {
     if ((e = cudaEventCreate(&c.ev0)) || (e = cudaEventCreate(&c.ev1))) return e;
   }
   cudaEventRecord(c.ev0, c.stream);
   ++c.launches;
-  const int occ = a.occupancy_override >= 0 ? a.occupancy_override : c.render_occupancy;
   unsigned long long* stats = reinterpret_cast<unsigned long long*>(c.flags.as<char>() + 64);
   if (occ == 5)
     render_kernel<5><<<grid, kRenderThreads, 0, c.stream>>>(k, g, c.spiral.as<char4>(),

@@ -52,15 +52,33 @@ __device__ __forceinline__ void s4_bind(Step4& s, SlotMem& m) {
   s.sv = &m.v[0][threadIdx.x];
 }
 
+// The larger of two (distance, slot) pairs, the left one on ties.
+__device__ __forceinline__ void max_left(float& d, int& i, float d2, int i2) {
+  const bool right = d2 > d;
+  d = right ? d2 : d;
+  i = right ? i2 : i;
+}
+
+// Search radius and first maximal slot (volumetric_nn8_reconstruction.cl:
+// 135-143), as a pairwise tournament: three levels instead of a chain of
+// eight; keeping the left pair on ties gives the first slot holding the
+// maximum, as the sequential scan does (distances are non-negative, so the
+// scan's start at 0 changes nothing).
 template <int J> __device__ __forceinline__ void s4_rescan(Step4& s) {
-  float r = 0.0f;
-  int m = 0;
+  float d[8];
 #pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const float d = s4_d(s, J, t);
-    if (d > r) m = t;
-    r = fmaxf(r, d);
-  }
+  for (int t = 0; t < 8; ++t) d[t] = s4_d(s, J, t);
+  int i0 = 0, i2 = 2, i4 = 4, i6 = 6;
+  float a0 = d[0], a2 = d[2], a4 = d[4], a6 = d[6];
+  max_left(a0, i0, d[1], 1);
+  max_left(a2, i2, d[3], 3);
+  max_left(a4, i4, d[5], 5);
+  max_left(a6, i6, d[7], 7);
+  max_left(a0, i0, a2, i2);
+  max_left(a4, i4, a6, i6);
+  max_left(a0, i0, a4, i4);
+  const float r = a0;
+  const int m = i0;
   s.R[J] = r;
   s.mi[J] = m;
   s.R2up[J] = __fmul_ru(r, r);
@@ -293,6 +311,20 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
     st.cells += na;
     st.cands += na * (uint32_t)max(be.y - be.x, 0);
     if (be.x >= be.y) continue;
+    {
+      // Every particle of the cell lies in its box (to within the rounding of
+      // the cell keys, which g.margin covers). If the box is farther from the
+      // points' bounding box than the largest threshold allows, no candidate
+      // of the cell can be inserted for any point: the cell is counted as
+      // visited, and its scan is skipped.
+      const float gx = fmaxf(fmaxf(qlo[0] - (ccx + g.half0), (ccx - g.half0) - qhi[0]) - g.margin,
+                             0.0f);
+      const float gy = fmaxf(fmaxf(qlo[1] - (ccy + g.half1), (ccy - g.half1) - qhi[1]) - g.margin,
+                             0.0f);
+      const float gz = fmaxf(fmaxf(qlo[2] - (ccz + g.half2), (ccz - g.half2) - qhi[2]) - g.margin,
+                             0.0f);
+      if ((gx * gx + gy * gy) + gz * gz > thrmax) continue;
+    }
     if (be.y - be.x > kPruneMin) {
       // Dense cell: candidates in ascending index order, 16 codes per chunk.
       // The sub-box mask follows the search radius as it shrinks while the
@@ -349,7 +381,12 @@ __device__ __forceinline__ void locate_axis(float q, float mn, float cs, float h
 }
 
 // nn8 walk of the 4 points of one step; the slots are left in s.
-template <bool kIdx>
+// kAxis: the caller guarantees lx == ly == 0 (a view along z). Then every
+// point's x is px + zq * 0 = px + 0, the same value for the 4 points whatever
+// their zq (zq * 0 is +0 for the positive distances along the ray, and NaN
+// for all 4 if the step is NaN), so the points share x and y without the
+// run-time test and only the shared-x/y walk is compiled.
+template <bool kIdx, bool kAxis = false>
 __device__ __forceinline__ void nn8_walk_step4(const GridView& g,
                                                const char4* __restrict__ spiral, float px,
                                                float py, float pz, float lx, float ly, float lz,
@@ -357,12 +394,13 @@ __device__ __forceinline__ void nn8_walk_step4(const GridView& g,
   int cx[4], cy[4], cz[4], sb[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    s.qx[j] = px + zq[j] * lx;
-    s.qy[j] = py + zq[j] * ly;
+    s.qx[j] = px + zq[kAxis ? 0 : j] * lx;
+    s.qy[j] = py + zq[kAxis ? 0 : j] * ly;
     s.qz[j] = pz + zq[j] * lz;
   }
-  const bool shared_xy = s.qx[0] == s.qx[1] && s.qx[0] == s.qx[2] && s.qx[0] == s.qx[3] &&
-                         s.qy[0] == s.qy[1] && s.qy[0] == s.qy[2] && s.qy[0] == s.qy[3];
+  const bool shared_xy = kAxis || (s.qx[0] == s.qx[1] && s.qx[0] == s.qx[2] &&
+                                   s.qx[0] == s.qx[3] && s.qy[0] == s.qy[1] &&
+                                   s.qy[0] == s.qy[2] && s.qy[0] == s.qy[3]);
   // points with bit-identical x and y (a view along z) share their x/y cell
   // and subcell: located once
   int cx0, sx0, cy0, sy0;
