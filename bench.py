@@ -798,6 +798,32 @@ def run_scale(args):
     ctx.close()
 
 
+def run_spectrum_probe(args):
+    """--spectrum-probe: one small 128-channel batched render (camera 16 of the
+    spectral workload, a 512^2 view with a 1.2 Mpc aperture, at half its side:
+    8,328 rays), three launches, for profiling the multi-channel kernel."""
+    import torch
+    import illcrawl_b200 as ilc
+    cells, xyz4 = make_inputs()
+    ctx = ilc.Context(0)
+    ctx.load_gaunt()
+    dev = torch.device("cuda", 0)
+    d_rho, d_u, d_xe = (torch.from_numpy(a).to(dev) for a in (cells.rho, cells.u, cells.xe))
+    q = ctx.xray_flux(d_rho, d_u, d_xe, REDSHIFT, DL, E_MIN, E_MAX, NUM_SAMPLES)
+    d_cells = torch.from_numpy(xyz4).to(dev)
+    ctx.setup_particles(torch.cat([d_cells[:, :3], q[:, None]], dim=1).contiguous())
+    tab = spectral_table(ctx, d_rho, d_u, d_xe)
+    spectral_schedule(ctx, ilc, tab, torch.cuda.get_device_name(dev), args)
+    job = [spectrum_jobs(ilc, 2)[16]]
+    out = []
+    for _ in range(3):
+        _, st = ctx.render_batched(tab, job)
+        out.append(st["kernel_ms"])
+    print(json.dumps({"spectrum_probe": {"rays": rays_of(job), "bins": 128,
+                                         "kernel_ms": out, "stats": st}}), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -831,6 +857,8 @@ def main():
                     help="camera plane position along z (profiling cases only)")
     ap.add_argument("--z-range", type=float, default=None,
                     help="integration depth in kpc (default: the 6 Mpc box; profiling only)")
+    ap.add_argument("--spectrum-probe", action="store_true",
+                    help="profiling only: three small 128-channel batched launches")
     ap.add_argument("--config", type=int, default=1, choices=[1, 4],
                     help="1: the band-map benchmark (default); 4: the 67 M-cell scale "
                          "workload, one GPU, one pass of each of its parts")
@@ -847,6 +875,9 @@ def main():
         return
     from illcrawl_b200 import build
     build.build()
+    if args.spectrum_probe:
+        run_spectrum_probe(args)
+        return
     if args.config == 4:
         if world > 1:
             raise SystemExit("--config 4 runs on one GPU")
