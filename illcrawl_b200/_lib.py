@@ -124,6 +124,9 @@ SIGNATURES = {
                                      _f64, Tolerance, _i32, _P, _P, _int, _P]),
     "ilc_kernel_launches": (_u64, [_P]),
     "ilc_grid_build_noalloc": (_int, [_P, _u64, _P, _P, _u64, _P, _P, _P]),
+    "ilc_device_alloc": (_int, [_P, _u64, _P]),
+    "ilc_device_free": (_int, [_P, _P]),
+    "ilc_copy": (_int, [_P, _P, _P, _u64]),
     "ilc_autotune_render": (_int, [_P, _P, _f64, Tolerance, _i32, _P, _i32, _P, _i32, _i32, _P,
                                    _P, _P]),
     "ilc_set_render_occupancy": (_int, [_P, _i32]),

@@ -1030,6 +1030,37 @@ ilc_status ilc_project_xray_flux(ilc_ctx* h, const float* cells, const float* rh
 
 uint64_t ilc_kernel_launches(const ilc_ctx* h) { return h ? h->c.launches : 0; }
 
+ilc_status ilc_device_alloc(ilc_ctx* h, uint64_t bytes, void** out) {
+  if (!h || !out) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  *out = nullptr;
+  if (bytes == 0) return ILC_OK;
+  cudaSetDevice(c.device);
+  ILC_CUDA(c, cudaMalloc(out, bytes), "device alloc");
+  return ILC_OK;
+}
+
+ilc_status ilc_device_free(ilc_ctx* h, void* p) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  if (!p) return ILC_OK;
+  Context& c = h->c;
+  cudaSetDevice(c.device);
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "device free");
+  ILC_CUDA(c, cudaFree(p), "device free");
+  return ILC_OK;
+}
+
+ilc_status ilc_copy(ilc_ctx* h, void* dst, const void* src, uint64_t bytes) {
+  if (!h) return ILC_ERR_INVALID_ARGUMENT;
+  Context& c = h->c;
+  if (bytes == 0) return ILC_OK;
+  if (!dst || !src) return fail(c, ILC_ERR_INVALID_ARGUMENT, "null array");
+  cudaSetDevice(c.device);
+  ILC_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c.stream), "copy");
+  ILC_CUDA(c, cudaStreamSynchronize(c.stream), "copy");
+  return ILC_OK;
+}
+
 ilc_status ilc_nn8_query_stats(ilc_ctx* h, uint64_t* cells_visited, uint64_t* candidates) {
   if (!h || !cells_visited || !candidates) return ILC_ERR_INVALID_ARGUMENT;
   Context& c = h->c;

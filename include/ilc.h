@@ -599,6 +599,19 @@ ilc_status ilc_grid_build_noalloc(const float* particles, uint64_t n, float* sor
 /* Number of kernels this context has launched so far. */
 uint64_t ilc_kernel_launches(const ilc_ctx* ctx);
 
+/* ---- device memory ----------------------------------------------------------
+ * Device memory on the context's device, for hosts that keep evaluation
+ * points and results on the device without linking the CUDA runtime
+ * themselves: the role of the cl::Buffer objects the reference's backends own
+ * and hand out (reconstruction_backend.hpp:43 retrieve_results,
+ * volumetric_reconstruction_backend_nn8.hpp:72-80 _evaluation_points /
+ * _results). ilc_device_free waits for the context's stream first.
+ * ilc_copy copies `bytes` between any two host or device pointers on the
+ * context's stream and waits for the copy. */
+ilc_status ilc_device_alloc(ilc_ctx* ctx, uint64_t bytes, void** out);
+ilc_status ilc_device_free(ilc_ctx* ctx, void* p);
+ilc_status ilc_copy(ilc_ctx* ctx, void* dst, const void* src, uint64_t bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,7 +3,9 @@
 // Header-only, over the C ABI of ilc.h. It mirrors:
 //   * reconstruction_backend / reconstruction_backends::nn8
 //     (reconstruction_backend.hpp:35-58, volumetric_reconstruction_backend_nn8.hpp:36-82):
-//     class nn8_cuda, with a device_view (pointer + count) in place of cl::Buffer;
+//     the abstract class reconstruction_backend and its implementation nn8_cuda,
+//     with device_buffer (device memory owned through the library) in place of
+//     cl::Buffer, so query results stay on the device as in the reference;
 //   * volumetric_integration::create_projection (volumetric_integration.cpp:32-88):
 //     function create_projection, which runs the whole RKF loop on the device.
 // Errors are reported as exceptions (ilc::error), as the reference's
@@ -54,55 +56,151 @@ template <class T> struct view {
   bool on_device = false;
 };
 
+// Device memory owned through the library (the role of cl::Buffer in the
+// reference's backends). Move-only.
+template <class T> class device_buffer {
+ public:
+  device_buffer() = default;
+  device_buffer(context& ctx, std::size_t n) : ctx_(&ctx) { resize(n); }
+  ~device_buffer() { release(); }
+  device_buffer(const device_buffer&) = delete;
+  device_buffer& operator=(const device_buffer&) = delete;
+  device_buffer(device_buffer&& o) noexcept : ctx_(o.ctx_), p_(o.p_), n_(o.n_) {
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  device_buffer& operator=(device_buffer&& o) noexcept {
+    if (this != &o) {
+      release();
+      ctx_ = o.ctx_; p_ = o.p_; n_ = o.n_;
+      o.p_ = nullptr;
+      o.n_ = 0;
+    }
+    return *this;
+  }
+  void bind(context& ctx) { ctx_ = &ctx; }
+  // Grow-only: keeps the allocation when n fits (contents are not kept on growth).
+  void resize(std::size_t n) {
+    if (n <= cap_) {
+      n_ = n;
+      return;
+    }
+    release();
+    void* p = nullptr;
+    ctx_->check(ilc_device_alloc(ctx_->get(), (uint64_t)(n * sizeof(T)), &p));
+    p_ = static_cast<T*>(p);
+    n_ = cap_ = n;
+  }
+  T* data() const { return p_; }
+  std::size_t size() const { return n_; }
+  view<const T> cview() const { return view<const T>{p_, n_, true}; }
+  void copy_from_host(const T* src, std::size_t n) {
+    resize(n);
+    ctx_->check(ilc_copy(ctx_->get(), p_, src, (uint64_t)(n * sizeof(T))));
+  }
+  std::vector<T> to_host() const {
+    std::vector<T> out(n_);
+    if (n_) ctx_->check(ilc_copy(ctx_->get(), out.data(), p_, (uint64_t)(n_ * sizeof(T))));
+    return out;
+  }
+
+ private:
+  void release() {
+    if (p_ && ctx_) ilc_device_free(ctx_->get(), p_);
+    p_ = nullptr;
+    n_ = cap_ = 0;
+  }
+  context* ctx_ = nullptr;
+  T* p_ = nullptr;
+  std::size_t n_ = 0, cap_ = 0;
+};
+
 // float4 particle record, the reference's device_vector4 (x, y, z, quantity).
 struct particle {
   float s[4];
 };
 
-// reconstruction_backends::nn8 over the CUDA context.
-class nn8_cuda {
+// reconstruction_backend (reconstruction_backend.hpp:35-58) with CUDA device
+// buffers in place of cl::Buffer and dataset names in place of H5::DataSet
+// handles: additional per-particle datasets arrive as float arrays in the
+// order get_required_additional_datasets names them.
+class reconstruction_backend {
  public:
-  explicit nn8_cuda(context& ctx) : ctx_(ctx) {}
-  virtual ~nn8_cuda() {}
+  using particle = ilc::particle;
+  virtual std::vector<std::string> get_required_additional_datasets() const = 0;
+  virtual const device_buffer<float>& retrieve_results() = 0;
+  virtual std::string get_backend_name() const = 0;
+  virtual void init_backend(std::size_t blocksize) = 0;
+  virtual void setup_particles(const std::vector<particle>& particles,
+                               const std::vector<view<const float>>& additional_datasets) = 0;
+  virtual void setup_evaluation_points(view<const float> evaluation_points,
+                                       std::size_t num_points) = 0;
+  virtual void run() = 0;
+  virtual ~reconstruction_backend() {}
+};
+
+// reconstruction_backends::nn8 (volumetric_reconstruction_backend_nn8.hpp:36-82,
+// volumetric_reconstruction_backend_nn8.cpp:26-141) over the CUDA context.
+// As in the reference, the results stay on the device: retrieve_results()
+// hands out the backend's own device buffer (one float per evaluation point),
+// valid until the next setup_evaluation_points; results_to_host() copies it.
+// Host evaluation points are staged into a device buffer once per
+// setup_evaluation_points; device points are borrowed, as the reference
+// borrows the caller's cl::Buffer.
+class nn8_cuda : public reconstruction_backend {
+ public:
+  explicit nn8_cuda(context& ctx) : ctx_(ctx), points_dev_(), result_() {
+    points_dev_.bind(ctx);
+    result_.bind(ctx);
+  }
 
   // No smoothing lengths or other per-particle datasets are needed
   // (volumetric_reconstruction_backend_nn8.cpp:32-35).
-  std::vector<std::string> get_required_additional_datasets() const { return {}; }
-  std::string get_backend_name() const { return "volumetric/nn8_cuda"; }
-  void init_backend(std::size_t blocksize) { blocksize_ = blocksize; }
+  std::vector<std::string> get_required_additional_datasets() const override { return {}; }
+  std::string get_backend_name() const override { return "volumetric/nn8_cuda"; }
+  void init_backend(std::size_t blocksize) override { blocksize_ = blocksize; }
 
-  void setup_particles(const std::vector<particle>& particles) {
+  void setup_particles(const std::vector<particle>& particles,
+                       const std::vector<view<const float>>& = {}) override {
     ctx_.check(ilc_nn8_setup_particles(ctx_.get(), &particles[0].s[0], particles.size(), 0));
   }
+  // Particles already on the device (float4 each), or on the host.
   void setup_particles(view<const float> particles_float4) {
     ctx_.check(ilc_nn8_setup_particles(ctx_.get(), particles_float4.ptr, particles_float4.n,
                                        particles_float4.on_device ? 1 : 0));
   }
 
-  // Borrowed until the next setup_evaluation_points, as the reference's cl::Buffer.
-  void setup_evaluation_points(view<const float> points_float4, std::size_t num_points) {
-    points_ = points_float4;
+  void setup_evaluation_points(view<const float> points_float4,
+                               std::size_t num_points) override {
+    if (points_float4.on_device) {
+      points_ = points_float4.ptr;
+    } else {
+      points_dev_.copy_from_host(points_float4.ptr, num_points * 4);
+      points_ = points_dev_.data();
+    }
     n_ = num_points;
     first_run_ = true;
-    result_.assign(num_points, 0.0f);
+    result_.resize(num_points);
   }
 
   // One particle block; later blocks merge into the running lists.
-  void run() {
-    ctx_.check(ilc_nn8_query(ctx_.get(), points_.ptr, n_, first_run_ ? 0 : 1, result_.data(),
-                             nullptr, nullptr, points_.on_device ? 1 : 0));
+  void run() override {
+    ctx_.check(ilc_nn8_query(ctx_.get(), points_, n_, first_run_ ? 0 : 1, result_.data(),
+                             nullptr, nullptr, 1));
     first_run_ = false;
   }
 
-  const std::vector<float>& retrieve_results() const { return result_; }
+  const device_buffer<float>& retrieve_results() override { return result_; }
+  std::vector<float> results_to_host() const { return result_.to_host(); }
 
  private:
   context& ctx_;
   std::size_t blocksize_ = 0;
-  view<const float> points_;
+  const float* points_ = nullptr;
   std::size_t n_ = 0;
   bool first_run_ = true;
-  std::vector<float> result_;
+  device_buffer<float> points_dev_;
+  device_buffer<float> result_;
 };
 
 // volumetric_integration::create_projection: output is num_pix_x * num_pix_y

@@ -16,15 +16,32 @@ int main() {
     std::uniform_real_distribution<float> u(0.f, 100.f);
     std::vector<ilc::particle> parts(20000);
     for (auto& p : parts) p = ilc::particle{{u(rng), u(rng), u(rng), 1.0f + u(rng) / 100.f}};
-    ilc::nn8_cuda backend(ctx);
+    // through the abstract interface, as the crawler holds its backend
+    ilc::nn8_cuda impl(ctx);
+    ilc::reconstruction_backend& backend = impl;
     backend.init_backend(40000000);
-    backend.setup_particles(parts);
+    backend.setup_particles(parts, {});
     std::vector<float> pts(4 * 1000);
     for (auto& v : pts) v = u(rng);
     backend.setup_evaluation_points(ilc::view<const float>{pts.data(), pts.size() / 4, false}, 1000);
     backend.run();
+    const ilc::device_buffer<float>& res = backend.retrieve_results();
+    if (res.size() != 1000 || res.data() == nullptr) {
+      std::printf("device result buffer missing\n");
+      return 1;
+    }
+    const std::vector<float> host_res = res.to_host();
+    // the same points already on the device: the results must not differ
+    ilc::device_buffer<float> dpts(ctx, pts.size());
+    dpts.copy_from_host(pts.data(), pts.size());
+    backend.setup_evaluation_points(ilc::view<const float>{dpts.data(), 1000, true}, 1000);
+    backend.run();
+    if (impl.results_to_host() != host_res) {
+      std::printf("device-point query differs from host-point query\n");
+      return 1;
+    }
     double sum = 0;
-    for (float v : backend.retrieve_results()) sum += v;
+    for (float v : host_res) sum += v;
     ilc_camera cam{{50, 50, 0}, {0, 0, 1}, 0.0, 100.0, 16, 16};
     std::vector<float> img;
     ilc::create_projection(ctx, cam, 100.0, 0.0, 1e-3, ilc_los_scaling{1.0, 1.0, ILC_DA_UNIT}, img);
@@ -41,7 +58,7 @@ int main() {
     const double centre[3] = {50, 50, 50}, extent[3] = {80, 80, 80}, period[3] = {100, 100, 100};
     std::vector<uint32_t> kept_index;
     auto kept = ilc::ingest_cells(ctx, xyz, q, centre, extent, period, 5.0, &kept_index);
-    backend.setup_particles(kept);
+    backend.setup_particles(kept, {});
     std::vector<float> slice;
     ilc::volumetric_slice(ctx, cam, 1.0, slice);
     for (float v : slice) sum += v;
