@@ -411,7 +411,24 @@ def accuracy_leg(img, g):
             "bit_exact_vs_oracle": same, "rays": len(pix),
             "vs_fp64_oracle_same_tol": rel_stats(raw, o64),
             "vs_fp64_converged_rtol1e-5": rel_stats(raw, conv),
-            "fp64_oracle_same_tol_vs_converged": rel_stats(o64, conv)}
+            "fp64_oracle_same_tol_vs_converged": rel_stats(o64, conv)}, conv
+
+
+def tolerance_leg(step_at, conv):
+    """The same map at tighter relative tolerances (outside the timed region):
+    kernel time and the sampled pixels' error against the converged FP64
+    render, i.e. what a per-pixel error bound of 1e-3 costs. step_at(rtol)
+    renders the map and returns (device image, stats)."""
+    import oracle
+    ocam = oracle.camera(*camera_args())
+    scale = float(np.float32(oracle.los_scale(ocam, DEPTH, 1.0, 1.0, 0)))
+    out = {}
+    for rtol in (5e-4, 2.5e-4):
+        img, st = step_at(rtol)
+        got = img.cpu().numpy().ravel()[sample_pixels()].astype(np.float64) / scale
+        out[f"rtol{rtol:g}"] = {"kernel_ms": st["kernel_ms"], "steps": st["steps"],
+                                "vs_fp64_converged_rtol1e-5": rel_stats(got, conv)}
+    return out
 
 
 def fixed_leg(ctx, ilc, torch, cam, flush, g):
@@ -431,6 +448,45 @@ def fixed_leg(ctx, ilc, torch, cam, flush, g):
             "mrays_per_s": NX * NY / (st["kernel_ms"] * 1e-3) / 1e6,
             "bit_exact_vs_oracle": int(np.sum(got.view(np.uint32) == o32.view(np.uint32))),
             "vs_fp64_replay": rel_stats(got, o64)}
+
+
+def query_leg(ctx, ilc, torch):
+    """The nn8 query workload of the projected-density cells (262,144 seeded
+    cells, NFW r_s 300 kpc in a 3 Mpc cube, q = rho): 2^20 uniform random
+    queries in the cube, device-resident, through ilc_nn8_query with the
+    one-thread-per-query walk and with the warp-per-query walk (cells and
+    candidates 32 at a time, hits by ballot). Device time of the query call
+    (CUDA events on the library's stream), best of 5 after 2 warm-ups; the two
+    engines' values compared bit for bit."""
+    from illcrawl_b200 import synthetic
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cells = synthetic.plain_density_cells()
+    ctx.setup_particles(torch.from_numpy(cells.xyzq(cells.rho)).to(dev))
+    rng = np.random.default_rng(20170)
+    q = np.zeros((1 << 20, 4), np.float32)
+    q[:, :3] = (rng.random((1 << 20, 3)) * cells.box).astype(np.float32)
+    dq = torch.from_numpy(q).to(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    out = {"workload": "2^20 uniform nn8 queries, 262,144 NFW cells in a 3 Mpc cube"}
+    vals = {}
+    for name, eng in (("thread", ilc.QUERY_THREAD), ("warp", ilc.QUERY_WARP)):
+        ctx.set_query_engine(eng)
+        times = []
+        for i in range(7):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            v = ctx.nn8_query(dq)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= 2:
+                times.append(e0.elapsed_time(e1))
+        vals[name] = v.cpu().numpy()
+        out[name] = {"ms": min(times), "mqueries_per_s": (1 << 20) / min(times) * 1e3 / 1e6}
+    ctx.set_query_engine(ilc.QUERY_THREAD)
+    out["bit_identical"] = bool(np.array_equal(vals["thread"].view(np.uint32),
+                                               vals["warp"].view(np.uint32)))
+    return out
 
 
 def bytes_provenance(stats):
@@ -625,7 +681,12 @@ def run_ours(args, rank, world, local_rank):
         cpu_v, t_fixed, t_render, g_oracle = cpu_baseline(cells, cores)
         cpu_info = {"grid_and_flux_s": t_fixed, "render_s": t_render}
     if g_oracle is not None and not args.no_accuracy:
-        extra["accuracy"] = accuracy_leg(d_img.cpu().numpy(), g_oracle)
+        extra["accuracy"], conv = accuracy_leg(d_img.cpu().numpy(), g_oracle)
+        extra["tighter_tolerance"] = tolerance_leg(
+            lambda rt: ctx.project_xray_flux(d_cells, d_rho, d_u, d_xe, cam, DEPTH, rel_tol=rt,
+                                             controller=ilc.CONTROLLER_FP64, e_min=E_MIN,
+                                             e_max=E_MAX, num_samples=NUM_SAMPLES,
+                                             scaling=scaling), conv)
         extra["fixed_2048"] = fixed_leg(ctx, ilc, torch, cam, flush, g_oracle)
     band_sched = tuned if tuned and "tile_w" in tuned else {"tile_w": 4, "occupancy": 4,
                                                              "z_window": 80.0}
@@ -634,6 +695,8 @@ def run_ours(args, rank, world, local_rank):
                                        gpu_name)
     if world == 1 and not args.no_adjoint:
         extra["adjoint"] = adjoint_leg(ctx, ilc, cells, args)
+    if world == 1 and not args.no_queries:
+        extra["nn8_queries"] = query_leg(ctx, ilc, torch)
     del g_oracle
     if rank != 0:
         ctx.close()
@@ -851,6 +914,8 @@ def main():
                     help="bins timed per camera in the plain per-(camera, bin) arm of the "
                          "full-size spectral comparison, scaled to 128")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
+    ap.add_argument("--no-queries", action="store_true",
+                    help="skip the 2^20-query nn8 leg (thread vs warp engine)")
     ap.add_argument("--autotune", action="store_true",
                     help="re-run the schedule autotuner and update the cache")
     ap.add_argument("--z-start", type=float, default=0.0,
