@@ -141,6 +141,110 @@ __global__ void scan_kernel(uint32_t* __restrict__ a, uint64_t m) {
   }
 }
 
+// Multi-block exclusive scan for long arrays (the radix histogram holds
+// 256 x tiles entries: 8.4 M at 67 M particles). Three coalesced passes:
+// per-chunk sums, a scan of the chunk sums by scan_kernel, then every chunk
+// scanned in place from its offset. Same result as scan_kernel (integer sums).
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 16;                           // consecutive entries per thread
+constexpr uint64_t kScanChunk = kScanThreads * kScanPer;  // 16,384 entries per block
+
+// Block-wide exclusive scan of one value per thread (1024 threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, off);
+    if (lane >= off) inc += t;
+  }
+  if (lane == 31) warp_tot[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = warp_tot[lane];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, w, off);
+      if (lane >= off) w += t;
+    }
+    warp_tot[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  return (warp ? warp_tot[warp - 1] : 0u) + inc - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_sums_kernel(const uint32_t* __restrict__ a,
+                                                                 uint64_t m,
+                                                                 uint32_t* __restrict__ sums) {
+  __shared__ uint32_t warp_tot[32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanChunk;
+  uint32_t s = 0;
+#pragma unroll
+  for (int it = 0; it < kScanPer; ++it) {
+    const uint64_t i = base + (uint64_t)it * kScanThreads + threadIdx.x;
+    if (i < m) s += a[i];
+  }
+  const uint32_t ex = block_exclusive_scan(s, warp_tot);
+  if (threadIdx.x == kScanThreads - 1) sums[blockIdx.x] = ex + s;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_chunks_kernel(uint32_t* __restrict__ a,
+                                                                   uint64_t m,
+                                                                   const uint32_t* __restrict__ offs) {
+  __shared__ uint32_t warp_tot[32];
+  const uint64_t b = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kScanPer;
+  uint32_t v[kScanPer];
+  if (b + kScanPer <= m) {  // 64-byte aligned: the array and every chunk start are
+    const uint4* p = reinterpret_cast<const uint4*>(a + b);
+#pragma unroll
+    for (int q = 0; q < kScanPer / 4; ++q) {
+      const uint4 t = p[q];
+      v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) v[k] = b + k < m ? a[b + k] : 0u;
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) s += v[k];
+  uint32_t run = block_exclusive_scan(s, warp_tot) + offs[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    const uint32_t t = v[k];
+    v[k] = run;
+    run += t;
+  }
+  if (b + kScanPer <= m) {
+    uint4* p = reinterpret_cast<uint4*>(a + b);
+#pragma unroll
+    for (int q = 0; q < kScanPer / 4; ++q)
+      p[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k)
+      if (b + k < m) a[b + k] = v[k];
+  }
+}
+
+// Number of chunk sums the multi-block scan of m entries needs.
+inline uint64_t scan_chunks(uint64_t m) { return (m + kScanChunk - 1) / kScanChunk; }
+
+// Exclusive scan of a[0, m) in place on stream st; `sums` holds
+// scan_chunks(m) entries (unused when m fits one chunk). a must be 16-byte
+// aligned. Returns the number of kernels launched.
+int scan_u32(uint32_t* a, uint64_t m, uint32_t* sums, cudaStream_t st) {
+  if (m <= kScanChunk) {
+    scan_kernel<<<1, 1024, 0, st>>>(a, m);
+    return 1;
+  }
+  const unsigned nb = (unsigned)scan_chunks(m);
+  scan_sums_kernel<<<nb, kScanThreads, 0, st>>>(a, m, sums);
+  scan_kernel<<<1, 1024, 0, st>>>(sums, nb);
+  scan_chunks_kernel<<<nb, kScanThreads, 0, st>>>(a, m, sums);
+  return 3;
+}
+
 // Stable scatter: items of a tile are ranked in index order (warp-contiguous
 // chunks of 256, lane-striped), per digit, then placed at the tile's scanned
 // digit offset.
@@ -294,7 +398,9 @@ cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n) {
       (e = c.flags.ensure(kFlagsBytes)))
     return e;
   const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
-  if ((e = c.hist.ensure(tiles * 256 * 4 + 64))) return e;
+  // histogram, then the scan's chunk sums
+  if ((e = c.hist.ensure(tiles * 256 * 4 + 4 * scan_chunks(tiles * 256) + 64))) return e;
+  uint32_t* chunk_sums = c.hist.as<uint32_t>() + tiles * 256;
   if ((e = cudaMemsetAsync(c.flags.p, 0, kFlagsBytes, c.stream))) return e;
 
   KeyGrid kg{g.min[0], g.min[1], g.min[2], g.cs[0], g.cs[1], g.cs[2], g.n[0], g.n[1], g.total};
@@ -310,8 +416,7 @@ cudaError_t grid_build_device(Context& c, const float4* in, uint64_t n) {
   for (int shift = 0; shift < bits; shift += 8) {
     radix_hist_kernel<<<(unsigned)tiles, kSortThreads, 0, c.stream>>>(
         ka, n, shift, (uint32_t)tiles, c.hist.as<uint32_t>());
-    scan_kernel<<<1, 1024, 0, c.stream>>>(c.hist.as<uint32_t>(), tiles * 256);
-    c.launches += 3;
+    c.launches += 2 + scan_u32(c.hist.as<uint32_t>(), tiles * 256, chunk_sums, c.stream);
     radix_scatter_kernel<<<(unsigned)tiles, kSortThreads, 0, c.stream>>>(
         ka, va, n, shift, (uint32_t)tiles, c.hist.as<uint32_t>(), kb, vb);
     if ((e = cudaGetLastError())) return e;
