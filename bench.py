@@ -126,11 +126,12 @@ def tune_schedule(ctx, cam, args, gpu_name):
     else:
         ctx.set_render_engine(ilc.ENGINE_PERSISTENT)
         key = base + "|persistent"
-        if args.z_window is not None or args.tile_w is not None:
+        if args.z_window is not None or args.tile_w is not None or args.occupancy is not None:
             tw = 4 if args.tile_w is None else args.tile_w
             zw = 80.0 if args.z_window is None else args.z_window
-            ctx.set_batch_schedule(tw, 4, zw, True)
-            return {"engine": "persistent", "tile_w": tw, "occupancy": 4,
+            oc = 4 if args.occupancy is None else args.occupancy
+            ctx.set_batch_schedule(tw, oc, zw, True)
+            return {"engine": "persistent", "tile_w": tw, "occupancy": oc,
                     "z_window": zw, "source": "command line"}
         if key in cache and not args.autotune:
             e = cache[key]
@@ -899,6 +900,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
     ap.add_argument("--z-window", type=float, default=None,
                     help="z window of the adaptive schedule in kpc (default: the tuned value)")
+    ap.add_argument("--occupancy", type=int, default=None, choices=[0, 3, 4, 5],
+                    help="blocks per SM of the persistent schedule (default: the tuned value)")
     ap.add_argument("--tile-w", type=int, default=None,
                     help="work-item width of the persistent schedule (default: the tuned value)")
     ap.add_argument("--engine", default="persistent", choices=["persistent", "grid"],
