@@ -177,10 +177,14 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
   // weights in the distance rows, indices in the value rows, sums in slot_ws
   __shared__ SlotMem slot_mem;
   __shared__ float slot_ws[kMulti ? 4 : 1][kBThreads];
+  // the block's work counters (steps, accepted, -, cells, candidates, max
+  // steps of a ray, rays at the step limit), added per tile: kept out of the
+  // registers the walk needs
+  __shared__ unsigned long long blk_stats[7];
+  if (threadIdx.x < 7) blk_stats[threadIdx.x] = 0ull;
   load_spiral(spiral, spiral_g);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tw = a.tile_w, th = a.tile_w > 0 ? 32 / a.tile_w : 1;
-  unsigned long long t_steps = 0, t_acc = 0, t_cells = 0, t_cands = 0, t_max = 0, t_lim = 0;
   float* wstate = kMulti ? a.state + ((size_t)blockIdx.x * kBThreads + (size_t)warp * 32) *
                                          4 * (size_t)a.V
                          : nullptr;
@@ -213,7 +217,7 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
     float z = 0.0f, h = 1.0f, I = 0.0f, k1 = 0.0f;
     float pts[4];
     rkf_points(0.0f, 1.0f, pts);
-    unsigned long long rs = 0, ra = 0;
+    uint32_t rs = 0, ra = 0;
     WalkStats ws;
     if (kMulti) {
       for (int i = lane; i < 32 * 4 * a.V; i += 32) wstate[i] = 0.0f;
@@ -229,7 +233,7 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
         continue;
       }
       if (run && z < len && z < wend && (int64_t)rs >= a.max_steps) {
-        t_lim += 1;
+        atomicAdd(&blk_stats[6], 1ull);
         run = false;
       }
       const bool go = run && z < len && z < wend;
@@ -397,30 +401,22 @@ batched_kernel(BatchK a, GridView g, const char4* __restrict__ spiral_g,
       }
       __syncwarp();
     }
-    t_steps += rs;
-    t_acc += ra;
-    t_cells += ws.cells;
-    t_cands += ws.cands;
-    t_max = max(t_max, rs);
+    atomicAdd(&blk_stats[0], (unsigned long long)rs);
+    atomicAdd(&blk_stats[1], (unsigned long long)ra);
+    atomicAdd(&blk_stats[3], (unsigned long long)ws.cells);
+    atomicAdd(&blk_stats[4], (unsigned long long)ws.cands);
+    atomicMax(&blk_stats[5], (unsigned long long)rs);
   }
-  if (t_lim) atomicOr(flags, FLAG_STEP_LIMIT);
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    t_steps += __shfl_xor_sync(kFull, t_steps, off);
-    t_acc += __shfl_xor_sync(kFull, t_acc, off);
-    t_cells += __shfl_xor_sync(kFull, t_cells, off);
-    t_cands += __shfl_xor_sync(kFull, t_cands, off);
-    t_lim += __shfl_xor_sync(kFull, t_lim, off);
-    t_max = max(t_max, __shfl_xor_sync(kFull, t_max, off));
-  }
-  if (lane == 0) {
-    atomicAdd(&stats[0], t_steps);
-    atomicAdd(&stats[1], t_acc);
-    atomicAdd(&stats[2], 4ull * t_steps);
-    atomicAdd(&stats[3], t_cells);
-    atomicAdd(&stats[4], t_cands);
-    atomicMax(&stats[5], t_max);
-    atomicAdd(&stats[6], t_lim);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (blk_stats[6]) atomicOr(flags, FLAG_STEP_LIMIT);
+    atomicAdd(&stats[0], blk_stats[0]);
+    atomicAdd(&stats[1], blk_stats[1]);
+    atomicAdd(&stats[2], 4ull * blk_stats[0]);
+    atomicAdd(&stats[3], blk_stats[3]);
+    atomicAdd(&stats[4], blk_stats[4]);
+    atomicMax(&stats[5], blk_stats[5]);
+    atomicAdd(&stats[6], blk_stats[6]);
   }
 }
 

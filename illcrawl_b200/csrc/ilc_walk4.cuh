@@ -34,10 +34,11 @@ struct Step4 {
   float qx[4], qy[4], qz[4];
   float* sd;      // this thread's distance column: sd[(j * 8 + t) * kSlotThreads]
   float* sv;      // this thread's value column
-  float R[4], R2up[4];
+  float R[4];
   float rr[4];    // (R + cell_radius)^2: the early-break threshold
   float crad;     // cell radius
-  int mi[4];      // first maximal slot; while R == FLT_MAX: the next empty slot
+  unsigned mi;    // per point j, bits 4j..4j+3: its first maximal slot; while
+                  // R == FLT_MAX: its next empty slot
 };
 
 __device__ __forceinline__ float& s4_d(const Step4& s, int j, int t) {
@@ -50,6 +51,10 @@ __device__ __forceinline__ float& s4_v(const Step4& s, int j, int t) {
 __device__ __forceinline__ void s4_bind(Step4& s, SlotMem& m) {
   s.sd = &m.d[0][threadIdx.x];
   s.sv = &m.v[0][threadIdx.x];
+}
+
+template <int J> __device__ __forceinline__ void s4_set_mi(Step4& s, unsigned k) {
+  s.mi = (s.mi & ~(15u << (4 * J))) | (k << (4 * J));
 }
 
 // The larger of two (distance, slot) pairs, the left one on ties.
@@ -80,8 +85,7 @@ template <int J> __device__ __forceinline__ void s4_rescan(Step4& s) {
   const float r = a0;
   const int m = i0;
   s.R[J] = r;
-  s.mi[J] = m;
-  s.R2up[J] = __fmul_ru(r, r);
+  s4_set_mi<J>(s, (unsigned)m);
   const float b = r + s.crad;
   s.rr[J] = b * b;
 }
@@ -93,10 +97,9 @@ template <int J> __device__ __forceinline__ void s4_init(Step4& s, float empty_v
     s4_v(s, J, t) = empty_value;
   }
   s.R[J] = FLT_MAX;
-  s.R2up[J] = __int_as_float(0x7f800000);
   const float b = FLT_MAX + s.crad;
   s.rr[J] = b * b;
-  s.mi[J] = 0;
+  s4_set_mi<J>(s, 0u);
 }
 
 // Insertion into point J's slots. While fewer than 8 slots are filled the
@@ -105,15 +108,21 @@ template <int J> __device__ __forceinline__ void s4_init(Step4& s, float empty_v
 // accepted candidate goes to slot k without a rescan; the 8th insertion
 // rescans. Afterwards: replace the first-max slot and rescan.
 template <int J> __device__ __forceinline__ void s4_insert(Step4& s, float dist, float val) {
-  const int k = s.mi[J];
+  const int k = (int)((s.mi >> (4 * J)) & 15u);
   s4_d(s, J, k) = dist;
   s4_v(s, J, k) = val;
   if (s.R[J] == FLT_MAX) {
-    s.mi[J] = k + 1;
+    s4_set_mi<J>(s, (unsigned)(k + 1));
     if (k == 7) s4_rescan<J>(s);
   } else {
     s4_rescan<J>(s);
   }
+}
+
+// Squared-distance threshold of point J: R*R rounded up (a squared distance
+// above it cannot give dist < R); +inf while R is FLT_MAX.
+template <int J> __device__ __forceinline__ float s4_r2up(const Step4& s) {
+  return __fmul_ru(s.R[J], s.R[J]);
 }
 
 // Candidate test of point J against its threshold thr: R2up (R*R rounded up:
@@ -126,7 +135,7 @@ __device__ __forceinline__ void s4_test(Step4& s, float& thr, float d2, float va
     const float dist = sqrtf(d2);
     if (dist < s.R[J]) {
       s4_insert<J>(s, dist, val);
-      thr = s.R2up[J];
+      thr = s4_r2up<J>(s);
     }
   }
 }
@@ -258,7 +267,7 @@ __device__ __forceinline__ void walk4(const GridView& g, const char4* __restrict
   unsigned act = mask;
   float thr[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) thr[j] = ((mask >> j) & 1u) ? s.R2up[j] : -1.0f;
+  for (int j = 0; j < 4; ++j) thr[j] = ((mask >> j) & 1u) ? __fmul_ru(s.R[j], s.R[j]) : -1.0f;
   // bounding box of the group's points (for the sub-box pruning)
   float qlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, qhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
 #pragma unroll

@@ -29,7 +29,10 @@ def _cells(seed, n, box=1000.0, r_s=100.0):
     return synthetic.small_cells(n, seed=seed, box=box, r_s=r_s)
 
 
-@pytest.mark.parametrize("n", [1, 2, 9, 1000, 50_000])
+# 131,073 particles: 65 sort tiles, a radix histogram of 16,640 entries, just
+# past the 16,384 the one-block scan takes (the multi-block scan's first size
+# with a partial second chunk); 1,000,003: a ragged last tile of 1,000,003 mod 2048.
+@pytest.mark.parametrize("n", [1, 2, 9, 1000, 50_000, 131_073, 1_000_003])
 def test_grid_build_bit_exact(ctx, oracle_mod, n):
     c = _cells(11, max(n, 1))
     pts = c.xyzq(c.rho)[:n]
