@@ -85,6 +85,7 @@ template <class T> class device_buffer {
       n_ = n;
       return;
     }
+    if (!ctx_) throw error(ILC_ERR_INVALID_ARGUMENT, "device_buffer has no context");
     release();
     void* p = nullptr;
     ctx_->check(ilc_device_alloc(ctx_->get(), (uint64_t)(n * sizeof(T)), &p));
