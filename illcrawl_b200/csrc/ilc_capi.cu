@@ -85,10 +85,14 @@ void make_grid_params(const float mn_f[3], const float mx_f[3], uint64_t n, Grid
   const double w = std::cbrt(cell_volume);
   g->total = 1;
   for (int i = 0; i < 3; ++i) {
-    g->n[i] = (int32_t)std::ceil((mx[i] - mn[i]) / w);
+    // cells per axis; 0 (rejected by the caller) when it does not fit an
+    // int32 or is not a positive number (the float -> int cast would be undefined)
+    const double nc = std::ceil((mx[i] - mn[i]) / w);
+    g->n[i] = (nc >= 1.0 && nc <= 2147483647.0) ? (int32_t)nc : 0;
     g->min[i] = (float)mn[i];
     g->cs[i] = (float)w;
     g->total *= (uint64_t)g->n[i];
+    if (g->total >= (1ull << 32)) g->total = 1ull << 32;  // rejected by the caller; no wrap
   }
 }
 

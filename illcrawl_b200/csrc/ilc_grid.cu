@@ -552,11 +552,13 @@ extern "C" ilc_status ilc_grid_build_noalloc(const float* particles, uint64_t n,
   int32_t nc[3];
   uint64_t total = 1;
   for (int k = 0; k < 3; ++k) {
-    nc[k] = (int32_t)std::ceil((mx[k] - mn[k]) / w);
+    const double c = std::ceil((mx[k] - mn[k]) / w);
+    nc[k] = (c >= 1.0 && c <= 2147483647.0) ? (int32_t)c : 0;  // 0: rejected below
     desc->min_corner[k] = (float)mn[k];
     desc->cell_sizes[k] = (float)w;
     desc->num_cells[k] = nc[k];
     total *= (uint64_t)(nc[k] > 0 ? nc[k] : 0);
+    if (total >= (1ull << 32)) total = 1ull << 32;  // rejected below; no wrap
   }
   desc->total_cells = total;
   desc->num_particles = n;

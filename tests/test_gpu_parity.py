@@ -69,6 +69,17 @@ def test_grid_rejects_nonfinite(ctx):
     assert e.value.status == 7
 
 
+def test_grid_rejects_too_many_cells(ctx):
+    """Particles 1e30 apart along x with no extent in y and z: the cells per
+    axis overflow an int32 (and the grid 2^32 cells), which is an error, not
+    a wrapped count."""
+    import illcrawl_b200 as ilc
+    p = np.float32([[0, 0, 0, 1], [1e30, 0, 0, 1], [5e29, 0, 0, 1]])
+    with pytest.raises(ilc.IlcError) as e:
+        ctx.setup_particles(p)
+    assert e.value.status == 8  # ILC_ERR_GRID_TOO_LARGE
+
+
 def test_nn8_density_workload_2p20_queries_bit_exact(ctx, oracle_mod):
     """262,144 density cells, 2^20 uniform random queries in the 3 Mpc cube:
     neighbour indices, distances and values bit-exact."""

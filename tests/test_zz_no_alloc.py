@@ -92,3 +92,20 @@ def test_noalloc_rejects_more_than_its_maximum(ctx):
                                     ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(d.data_ptr()),
                                     8, ctypes.c_void_p(d.data_ptr()), ctypes.byref(desc), None)
     assert st == 1
+
+
+def test_noalloc_rejects_a_grid_beyond_2_32_cells(ctx):
+    """Particles 1e30 apart along x: the cells per axis do not fit an int32;
+    the call reports ILC_ERR_GRID_TOO_LARGE before it writes any output."""
+    import torch
+    import illcrawl_b200 as ilc
+    lib = ctx.L
+    pts = torch.tensor([[0, 0, 0, 1], [1e30, 0, 0, 1], [5e29, 0, 0, 1]], dtype=torch.float32,
+                       device="cuda:0")
+    out = torch.zeros((8, 4), dtype=torch.float32, device="cuda:0")
+    desc = ilc._lib.GridDesc()
+    st = lib.ilc_grid_build_noalloc(ctypes.c_void_p(pts.data_ptr()), 3,
+                                    ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                    8, ctypes.c_void_p(out.data_ptr()), ctypes.byref(desc), None)
+    assert st == 8  # ILC_ERR_GRID_TOO_LARGE
+    assert torch.count_nonzero(out).item() == 0
