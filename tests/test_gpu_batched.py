@@ -178,4 +178,5 @@ def test_spectrum_table_and_accuracy_vs_fp64(ctx, oracle_mod, gaunt_table):
     ok = ref > 0
     rel = np.abs(got[ok] - ref[ok]) / ref[ok]
     print("spectrum vs FP64 per-bin: median", np.median(rel), "max", rel.max())
-    assert np.median(rel) < 2e-3 and np.quantile(rel, 0.9) < 2e-3 and rel.max() < 1e-2
+    # within 2 x rtol per pixel and bin (measured: median 6.0e-4, max 1.6e-3)
+    assert np.median(rel) < 1e-3 and rel.max() < 2e-3

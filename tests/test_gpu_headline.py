@@ -9,6 +9,8 @@ FP64 step controller, and the same map with a fixed 2048-step sequence.
   pixels bit-exact against the oracle, and their error against the FP64
   oracle at the same tolerance and against a converged FP64 render
   (rtol 1e-5);
+* the same map at rtol 5e-4: the sampled pixels bit-exact against the oracle
+  and every one within 1e-3 of the converged FP64 render;
 * per-ray work counters (steps, cells visited, candidates tested) of the same
   256 rays equal the oracle's counts committed in baseline/bytes_cfg1.json,
   from which the benchmark's algorithmic bytes follow; the one-block-per-tile
@@ -72,6 +74,14 @@ def band_map(ctx, band):
     return img.cpu().numpy(), st
 
 
+@pytest.fixture(scope="module")
+def converged(band, oracle_mod):
+    """The 256 sampled pixels rendered by the FP64 oracle at rtol 1e-5 (unscaled)."""
+    g = band[3]
+    conv, *_ = g.render(oracle_mod.camera(*CAM), BOX, 0.0, 1e-5, mode=2, pix=sample_pixels())
+    return np.asarray(conv, np.float64)
+
+
 def test_band_map_cells_and_grid_bit_exact(ctx, band):
     cells, q, oq, g = band
     assert same_bits(q, oq)
@@ -87,7 +97,8 @@ def test_band_map_cells_and_grid_bit_exact(ctx, band):
     assert np.array_equal(rsrt.view(np.uint32), osrt.view(np.uint32))
 
 
-def test_band_map_sampled_pixels_bit_exact_and_error_vs_fp64(band, band_map, oracle_mod):
+def test_band_map_sampled_pixels_bit_exact_and_error_vs_fp64(band, band_map, oracle_mod,
+                                                             converged):
     cells, q, oq, g = band
     img, st = band_map
     ocam = oracle_mod.camera(*CAM)
@@ -99,7 +110,7 @@ def test_band_map_sampled_pixels_bit_exact_and_error_vs_fp64(band, band_map, ora
     assert same_bits(got, (out * scale).astype(np.float32))
     raw = got.astype(np.float64) / float(scale)
     o64, *_ = g.render(ocam, BOX, 0.0, REL_TOL, mode=2, pix=pix)
-    conv, *_ = g.render(ocam, BOX, 0.0, 1e-5, mode=2, pix=pix)
+    conv = converged
     e_same = rel_stats(raw, o64)
     e_conv = rel_stats(raw, conv)
     e_o64 = rel_stats(o64, conv)
@@ -113,6 +124,33 @@ def test_band_map_sampled_pixels_bit_exact_and_error_vs_fp64(band, band_map, ora
     assert e_conv["median"] < 1e-3 and e_conv["p90"] < 2 * REL_TOL
     assert e_conv["max"] < 1.5 * max(e_o64["max"], REL_TOL)
     assert e_same["max"] < 5 * REL_TOL
+
+
+def test_band_map_per_pixel_error_below_1e3_at_rtol_5e4(ctx, band, oracle_mod, converged):
+    """A per-pixel error bound of 1e-3 against the converged integral needs a
+    tighter tolerance than 1e-3 (the adaptive method's own error at 1e-3 is up
+    to ~2e-3, for the FP64 oracle too): at rtol 5e-4 the map's sampled pixels
+    are bit-exact against the oracle and every one is within 1e-3 of the
+    converged FP64 render."""
+    import torch
+    import illcrawl_b200 as ilc
+    cells, q, oq, g = band
+    dev = torch.device("cuda", 0)
+    d_cells = torch.from_numpy(cells.xyzq(np.zeros(cells.n, np.float32))).to(dev)
+    d_rho, d_u, d_xe = (torch.from_numpy(a).to(dev) for a in (cells.rho, cells.u, cells.xe))
+    img, st = ctx.project_xray_flux(d_cells, d_rho, d_u, d_xe, ilc.camera(*CAM), BOX,
+                                    rel_tol=5e-4, controller=ilc.CONTROLLER_FP64,
+                                    e_min=EMIN, e_max=EMAX, num_samples=NS,
+                                    scaling=ilc.LosScaling(1.0, 1.0, ilc.DA_PIXEL_AREA))
+    ocam = oracle_mod.camera(*CAM)
+    pix = sample_pixels()
+    out, *_ = g.render(ocam, BOX, 0.0, 5e-4, mode=1, pix=pix)
+    scale = oracle_mod.los_scale(ocam, BOX, 1.0, 1.0, 0)
+    got = img.cpu().numpy().ravel()[pix]
+    assert same_bits(got, (out * scale).astype(np.float32))
+    e = rel_stats(got.astype(np.float64) / float(scale), converged)
+    print("rtol 5e-4 vs converged FP64:", e)
+    assert e["max"] < 1e-3
 
 
 def test_band_map_ray_counters_match_oracle_bytes(ctx, band, band_map):
