@@ -125,10 +125,9 @@ template <int J> __device__ __forceinline__ float s4_r2up(const Step4& s) {
   return __fmul_ru(s.R[J], s.R[J]);
 }
 
-// Candidate test of point J against its threshold thr: R2up (R*R rounded up:
-// a squared distance above it cannot give dist < R) while J takes part in the
-// walk, -1 once it has left it (no squared distance passes). thr follows R2up
-// through insertions.
+// Candidate test of point J against its threshold thr: s4_r2up while J takes
+// part in the walk, -1 once it has left it (no squared distance passes). thr
+// follows R through insertions.
 template <int J>
 __device__ __forceinline__ void s4_test(Step4& s, float& thr, float d2, float val) {
   if (d2 <= thr) {
