@@ -15,10 +15,12 @@
 //   X-ray quantities ...... quantities.cl:29-136,156-239,354-430,701-711
 //   Gaunt lookup .......... tabulated_function.cl:26-59, gaunt_factor.cpp:30-41
 //
-// Parity status. The reference ships no tests, golden vectors or fixtures for
-// this path. The two reference-pinned artefacts are the spiral table (checked
-// for equality against the reference file) and the Gaunt table (the reference
-// data file itself). Everything else is pinned to the op order declared here:
+// Parity status: parity unpinned. The reference ships no tests, golden vectors
+// or fixtures for this path, and its OpenCL kernels cannot be run here. The
+// reference-pinned artefacts are its tables: the spiral table (checked for
+// equality against the reference file), the Gaunt table (the reference data
+// file itself) and the Chandra ARF (extracted from the reference source into
+// a test fixture). Everything else is pinned to the op order declared here:
 // every expression is evaluated left to right exactly as written in the OpenCL
 // source, with no contraction into FMA except where the source calls fma()
 // (compile with -ffp-contract=off). Declared deviations from the OpenCL text:
